@@ -1,0 +1,277 @@
+/*
+ * rayon_b200.h - C-ABI of the B200 path-tracing render path.
+ *
+ * Two groups of entry points:
+ *
+ *  1. The drop-in group. Same names, argument lists and semantics as the
+ *     extern "C" block of RayON's CUDA renderer
+ *     (src/rayon/gpu_renderers/renderer_cuda_device.cuh:8-67), so the
+ *     unmodified host renderers (renderer_cuda_host.hpp,
+ *     renderer_cuda_progressive_host.hpp) link against this library in place
+ *     of the reference's .cu objects. Like the reference these return no
+ *     status; failures are recorded and readable through rb_last_error().
+ *
+ *  2. The rb_* group: scene construction (the SceneDescription builder
+ *     interface and its SAH BVH build), primary-hit queries, the batched
+ *     multi-job wavefront engine and the serving loop. These return
+ *     rb_status codes (0 = success, negative = error) and take an explicit
+ *     CUDA stream (passed as void*, NULL = legacy default stream).
+ *
+ * No torch types cross this boundary: plain pointers, sizes and PODs.
+ */
+#ifndef RAYON_B200_H
+#define RAYON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+namespace CudaScene { struct Scene; }
+typedef CudaScene::Scene rb_cuda_scene;
+extern "C" {
+#define RB_DEFAULT(x) = x
+#else
+typedef struct CudaScene_Scene rb_cuda_scene;
+#define RB_DEFAULT(x)
+#include <stdbool.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum rb_status {
+  RB_OK = 0,
+  RB_ERR_INVALID_ARG = -1,
+  RB_ERR_CUDA = -2,
+  RB_ERR_OUT_OF_MEMORY = -3,
+  RB_ERR_NOT_FOUND = -4,
+  RB_ERR_CAPACITY = -5,   /* admission refused: slot or memory budget */
+  RB_ERR_STATE = -6,      /* call made in the wrong state */
+  RB_ERR_UNSUPPORTED = -7
+} rb_status;
+
+/* Last error message of the calling thread ("" when none). */
+const char *rb_last_error(void);
+/* Library version string. */
+const char *rb_version(void);
+
+/* ======================================================================== */
+/* 1. Drop-in group (renderer_cuda_device.cuh:8-67)                          */
+/* ======================================================================== */
+
+/* Replaces initCudaStreams / cleanupCudaStreams
+ * (renderer_cuda_device.cuh:12-13; renderer_cuda_device.cu:35-54):
+ * create / destroy the display stream and its pinned staging buffer. */
+void initCudaStreams(void);
+void cleanupCudaStreams(void);
+
+/* Replaces renderPixelsCUDAAccumulative (renderer_cuda_device.cuh:18-24,
+ * renderer_cuda_device.cu:157-322). Adds samples_to_add samples per pixel to
+ * the accumulation buffer behind *d_accum_buffer_ptr (allocated on first use;
+ * uploaded from the host float3 accum_buffer when that is non-NULL, zeroed
+ * otherwise; downloaded into accum_buffer after every call when non-NULL).
+ * `image` is unused, as in the reference. Returns W*H*samples_to_add, or 0
+ * when scene is NULL or the call failed (see rb_last_error()). */
+unsigned long long renderPixelsCUDAAccumulative(
+    unsigned char *image, float *accum_buffer, rb_cuda_scene *scene, int width, int height,
+    double cam_center_x, double cam_center_y, double cam_center_z, double pixel00_x,
+    double pixel00_y, double pixel00_z, double delta_u_x, double delta_u_y, double delta_u_z,
+    double delta_v_x, double delta_v_y, double delta_v_z, int samples_to_add,
+    int total_samples_so_far, int max_depth, void **d_rand_states_ptr,
+    void **d_accum_buffer_ptr, double cam_u_x, double cam_u_y, double cam_u_z, double cam_v_x,
+    double cam_v_y, double cam_v_z, void *d_pixel_sample_counts RB_DEFAULT(NULL),
+    int min_adaptive_samples RB_DEFAULT(32), float adaptive_threshold RB_DEFAULT(0.01f));
+
+/* Replace freeDeviceRandomStates / freeDeviceAccumBuffer / resetDeviceAccumBuffer
+ * (renderer_cuda_device.cuh:27-33; renderer_cuda_device.cu:108-130). */
+void freeDeviceRandomStates(void *d_rand_states);
+void freeDeviceAccumBuffer(void *d_accum_buffer);
+void resetDeviceAccumBuffer(void *d_accum_buffer, int num_pixels);
+
+/* Replace the global shading setters (renderer_cuda_device.cuh:36-50;
+ * renderer_cuda_device.cu:57-79). Defaults match the reference's
+ * __constant__ initialisers (renderer_cuda_device.cu:18-26): light 1.0,
+ * background 1.0, metal fuzziness 0.8, glass IOR 1.5, DOF off, aperture 0.1
+ * (a disk radius), focus distance 10. */
+void setLightIntensity(float intensity);
+void setBackgroundIntensity(float intensity);
+void setMetalFuzziness(float fuzziness);
+void setGlassRefractionIndex(float index);
+void setDOFEnabled(bool enabled);
+void setDOFAperture(float aperture);
+void setDOFFocusDistance(float distance);
+
+/* Replaces convertAccumToDisplayCUDA (renderer_cuda_device.cuh:54-55;
+ * renderer_cuda_device.cu:340-393): sum/spp -> gamma -> clamp 0.999 -> u8. */
+void convertAccumToDisplayCUDA(void *d_accum_buffer, unsigned char *display_image, int width,
+                               int height, int channels, int num_samples, float gamma,
+                               void *d_pixel_sample_counts RB_DEFAULT(NULL));
+
+/* Replace the adaptive-sampling buffer helpers (renderer_cuda_device.cuh:58-63;
+ * renderer_cuda_device.cu:397-437). countConvergedPixels reduces on the device
+ * and copies back one integer. */
+void allocateAdaptiveBuffer(void **d_pixel_sample_counts, int num_pixels);
+void resetAdaptiveBuffer(void *d_pixel_sample_counts, int num_pixels);
+void freeAdaptiveBuffer(void *d_pixel_sample_counts);
+int countConvergedPixels(void *d_pixel_sample_counts, int num_pixels);
+
+/* Replaces renderSampleHeatmapCUDA (renderer_cuda_device.cuh:66-67;
+ * renderer_cuda_device.cu:440-478). */
+void renderSampleHeatmapCUDA(void *d_pixel_sample_counts, unsigned char *display_image, int width,
+                             int height, int channels, int max_samples_for_scale);
+
+/* ======================================================================== */
+/* 2. Scene description (host, FP64)                                         */
+/* ======================================================================== */
+
+/* Numbering of Scene::MaterialType (scene_description.hpp:29-43). */
+typedef enum rb_material_type {
+  RB_MAT_LAMBERTIAN = 0, RB_MAT_METAL, RB_MAT_MIRROR, RB_MAT_ROUGH_MIRROR, RB_MAT_GLASS,
+  RB_MAT_DIELECTRIC, RB_MAT_LIGHT, RB_MAT_CONSTANT, RB_MAT_SHOW_NORMALS, RB_MAT_SDF_MATERIAL,
+  RB_MAT_ANISOTROPIC_METAL, RB_MAT_THIN_FILM, RB_MAT_CLEAR_COAT
+} rb_material_type;
+
+/* Numbering of Scene::GeometryType (scene_description.hpp:252-260). */
+typedef enum rb_geometry_type {
+  RB_GEOM_SPHERE = 0, RB_GEOM_RECTANGLE, RB_GEOM_CUBE, RB_GEOM_DISPLACED_SPHERE,
+  RB_GEOM_TRIANGLE, RB_GEOM_TRIANGLE_MESH, RB_GEOM_SDF_PRIMITIVE
+} rb_geometry_type;
+
+/* Numbering of Scene::SDFType (scene_description.hpp:296-309); ROUND_BOX is
+ * an addition (a box with rounded edges, parameters = half extents, radius in
+ * `rotation[0]`-independent field `round_radius`). */
+typedef enum rb_sdf_type {
+  RB_SDF_SPHERE = 0, RB_SDF_BOX, RB_SDF_TORUS, RB_SDF_CAPSULE, RB_SDF_CYLINDER, RB_SDF_PLANE,
+  RB_SDF_MANDELBULB, RB_SDF_DEATH_STAR, RB_SDF_CUT_HOLLOW_SPHERE, RB_SDF_OCTAHEDRON,
+  RB_SDF_PYRAMID, RB_SDF_CUSTOM, RB_SDF_ROUND_BOX = 32
+} rb_sdf_type;
+
+/* Mirrors Scene::MaterialDesc (scene_description.hpp:58-101): vectors FP64,
+ * scalars FP32. rb_material_default() gives MaterialDesc()'s defaults. */
+typedef struct rb_material_desc {
+  int32_t type;
+  double albedo[3];
+  double emission[3];
+  float roughness, metallic, refractive_index, transmission, anisotropy;
+  double eta[3];
+  double k[3];
+  int32_t texture_id;
+  float film_thickness, film_ior;
+  int32_t pattern;
+  double pattern_color[3];
+  float pattern_param1, pattern_param2;
+} rb_material_desc;
+
+void rb_material_default(rb_material_desc *out);
+
+typedef struct rb_scene_desc rb_scene_desc; /* opaque host scene */
+
+rb_scene_desc *rb_scene_create(void);
+void rb_scene_destroy(rb_scene_desc *s);
+
+/* Builder interface, after SceneDescription (scene_description.hpp:487-711).
+ * Bounds are computed exactly as the reference computes them (FP64; triangle
+ * boxes padded by 1e-4). Geometry adders return the geometry index. */
+int rb_scene_add_material(rb_scene_desc *s, const rb_material_desc *m);
+int rb_scene_add_sphere(rb_scene_desc *s, const double center[3], double radius, int mat_id);
+int rb_scene_add_displaced_sphere(rb_scene_desc *s, const double center[3], double radius,
+                                  int mat_id, float displacement_scale, int pattern_type);
+int rb_scene_add_rectangle(rb_scene_desc *s, const double corner[3], const double u[3],
+                           const double v[3], int mat_id);
+int rb_scene_add_triangle(rb_scene_desc *s, const double v0[3], const double v1[3],
+                          const double v2[3], int mat_id);
+int rb_scene_add_triangle_with_normals(rb_scene_desc *s, const double v0[3], const double v1[3],
+                                       const double v2[3], const double n0[3],
+                                       const double n1[3], const double n2[3], int mat_id);
+int rb_scene_add_sdf(rb_scene_desc *s, int sdf_type, const double position[3],
+                     const double params[3], const double rotation[3], int mat_id);
+/* Bulk adders (same per-item semantics; n items, row-major):
+ * spheres: cr = n x 4 (cx, cy, cz, r); triangles: v = n x 9, nrm = n x 9 or NULL.
+ * mat_ids may be NULL (then mat_id is used for all). Return first index. */
+int64_t rb_scene_add_spheres(rb_scene_desc *s, const double *cr, const int32_t *mat_ids,
+                             int mat_id, int64_t n);
+int64_t rb_scene_add_triangles(rb_scene_desc *s, const double *v, const double *nrm,
+                               const int32_t *mat_ids, int mat_id, int64_t n);
+int rb_scene_set_visible(rb_scene_desc *s, int64_t geom_index, int visible);
+int64_t rb_scene_num_geometries(const rb_scene_desc *s);
+int rb_scene_num_materials(const rb_scene_desc *s);
+/* Smooth-union blend radius for the SDF primitives of this scene (0 = hard union). */
+int rb_scene_set_sdf_blend(rb_scene_desc *s, float k, int max_steps, float epsilon);
+
+/* SAH BVH build. Replaces SceneDescription::buildBVH
+ * (scene_description.hpp:717-778, 793-925) with the same node array, the same
+ * pre-order numbering and the same leaf-order geometry permutation for
+ * max_leaf = 4, built in parallel across subtrees with `threads` host threads
+ * (0 = all cores). max_leaf other than 4 is the tunable variant. */
+int rb_scene_build_bvh(rb_scene_desc *s);
+int rb_scene_build_bvh_ex(rb_scene_desc *s, int max_leaf, int threads);
+
+/* Host BVH node export (for parity): arrays of length rb_scene_num_bvh_nodes.
+ * Any pointer may be NULL. bounds = n x 6 (min xyz, max xyz) FP64. a/b =
+ * left/right child (interior) or first_geom_idx/geom_count (leaf). */
+int64_t rb_scene_num_bvh_nodes(const rb_scene_desc *s);
+int rb_scene_bvh_root(const rb_scene_desc *s);
+int rb_scene_export_bvh(const rb_scene_desc *s, double *bounds, int32_t *a, int32_t *b,
+                        uint8_t *is_leaf, uint8_t *split_axis);
+/* Original insertion index of the geometry now at each position (n). */
+int rb_scene_export_order(const rb_scene_desc *s, int64_t *orig_index);
+/* Geometry export (post-reorder), for the oracle: n x 20 doubles per item:
+ * [type, material_id, visible, has_normals, p0..p15] where p holds the
+ * type's parameters (sphere: c, r; rect: corner, u, v; tri: v0, v1, v2, n0,
+ * n1, n2 truncated to 16 -> see rb_scene_export_geometry_full). */
+int rb_scene_export_geometry_full(const rb_scene_desc *s, double *out /* n x 32 */);
+int rb_scene_export_materials(const rb_scene_desc *s, rb_material_desc *out);
+
+/* Camera frame. Replaces CameraBase::initialize (camera_base.hpp:76-99),
+ * FP64. out: center, pixel00, delta_u, delta_v, u, v, w (7 x 3 doubles). */
+void rb_camera_frame(const double look_from[3], const double look_at[3], const double vup[3],
+                     double vfov_deg, int width, int height, double out[21]);
+
+/* ======================================================================== */
+/* 3. Device scene                                                           */
+/* ======================================================================== */
+
+typedef struct rb_upload_opts {
+  int quantized_bvh;   /* 1: 8-bit child bounds relative to the parent */
+  int use_bvh;         /* 0: linear scan (reference use_bvh == false)   */
+  int reserved[6];
+} rb_upload_opts;
+
+/* Upload to the current device. Returns an opaque device-scene handle that is
+ * also accepted wherever the drop-in group takes a CudaScene::Scene*. */
+rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opts, void *stream);
+void rb_scene_free_device(rb_cuda_scene *scene);
+/* Device bytes held by a device scene. */
+int64_t rb_scene_device_bytes(const rb_cuda_scene *scene);
+
+/* Primary hits: pixel-centre rays (no jitter, no DOF), closest hit over the
+ * device BVH; ids[w*h] = leaf-order geometry index or -1; t may be NULL.
+ * ids / t are DEVICE pointers. */
+int rb_primary_hits(const rb_cuda_scene *scene, int width, int height, const double frame[21],
+                    int32_t *ids, float *t, void *stream);
+
+/* Global options of the drop-in group beyond the reference's setters. */
+typedef struct rb_render_opts {
+  int nee;            /* 1: next-event estimation with MIS on area lights   */
+  int kahan;          /* 1: Kahan-compensated FP32 accumulation (default 1) */
+  uint32_t seed;      /* RNG seed of the per-path counter-based streams     */
+  int block_x, block_y; /* launch shape of the per-pixel kernel (0 = tuned) */
+  int reserved[4];
+} rb_render_opts;
+void rb_get_render_opts(rb_render_opts *out);
+void rb_set_render_opts(const rb_render_opts *in);
+
+/* Device-resident accumulation into caller-owned DEVICE buffers (no lazy
+ * allocation, no host copies): accum = w*h float4 sums, comp = w*h float4
+ * Kahan compensation or NULL. sample_base = index of the first sample (the
+ * counter-based RNG key). counters (device, may be NULL) receives
+ * [segments, paths] as two uint64 added atomically. */
+int rb_render_accumulate(const rb_cuda_scene *scene, int width, int height, const double frame[21],
+                         int samples_to_add, int sample_base, int max_depth, float *accum,
+                         float *comp, uint64_t *counters, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#undef RB_DEFAULT
+#endif /* RAYON_B200_H */

@@ -1,0 +1,501 @@
+// Device side of the B200 render path: layout, intersection, traversal,
+// surface reconstruction and material scatter.
+//
+// Arithmetic that decides WHICH primitive a ray hits (box slabs, sphere,
+// quad and triangle tests, the closest-hit update rule and the traversal
+// order) is written operation for operation as in
+// src/rayon/gpu_renderers/cuda_raytracer.cuh:154-347, 487-602 and compiled
+// with the same fast-math flags, so primary-hit ids are bit-exact against
+// the reference. Everything after the hit (shading, sampling) is this
+// project's own and is checked statistically against the FP64 oracle.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rb_rng.h"
+
+namespace rbd {
+
+// ---------------------------------------------------------------------------
+// float3 algebra (expression shapes follow cuda_float3.cuh:41-96)
+// ---------------------------------------------------------------------------
+struct f3 {
+  float x, y, z;
+  __host__ __device__ __forceinline__ f3() {}
+  __host__ __device__ __forceinline__ f3(float a, float b, float c) : x(a), y(b), z(c) {}
+  __device__ __forceinline__ f3 operator+(const f3 &o) const { return f3(x + o.x, y + o.y, z + o.z); }
+  __device__ __forceinline__ f3 operator-(const f3 &o) const { return f3(x - o.x, y - o.y, z - o.z); }
+  __device__ __forceinline__ f3 operator*(float t) const { return f3(x * t, y * t, z * t); }
+  __device__ __forceinline__ f3 operator*(const f3 &o) const { return f3(x * o.x, y * o.y, z * o.z); }
+  __device__ __forceinline__ f3 operator/(float t) const { return f3(x / t, y / t, z / t); }
+  __device__ __forceinline__ f3 operator-() const { return f3(-x, -y, -z); }
+  __device__ __forceinline__ float length() const { return sqrtf(x * x + y * y + z * z); }
+  __device__ __forceinline__ float length_squared() const { return x * x + y * y + z * z; }
+};
+__device__ __forceinline__ f3 operator*(float t, const f3 &v) { return v * t; }
+__device__ __forceinline__ float dot(const f3 &a, const f3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(const f3 &a, const f3 &b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ f3 normalize(const f3 &v) { return v / v.length(); }
+__device__ __forceinline__ f3 mk(float4 v) { return f3(v.x, v.y, v.z); }
+
+struct Ray {
+  f3 o, d;
+  __device__ __forceinline__ f3 at(float t) const { return o + t * d; }
+};
+
+// ---------------------------------------------------------------------------
+// Device layout
+// ---------------------------------------------------------------------------
+// Primitive record: 3 x float4 = 48 B. Word 11 is the tag:
+//   bits 0-2 kind, bit 3 visible, bit 4 has vertex normals, bits 8-31 material.
+//   SPHERE / DISPLACED: f0 = (centre, radius)
+//   RECT:               f0 = (corner, u.x) f1 = (u.y, u.z, v.x, v.y) f2.x = v.z
+//   TRI:                f0 = (v0, e1.x)    f1 = (e1.y, e1.z, e2.x, e2.y) f2.x = e2.z
+//   SDF:                f0 = (bounding centre, bounding radius), f1.x = index into sdf table
+enum PrimKind : uint32_t { PK_SPHERE = 0, PK_RECT = 1, PK_TRI = 2, PK_DISPLACED = 3, PK_SDF = 4, PK_NONE = 7 };
+__device__ __host__ __forceinline__ uint32_t tag_kind(uint32_t t) { return t & 7u; }
+__device__ __host__ __forceinline__ bool tag_visible(uint32_t t) { return (t >> 3) & 1u; }
+__device__ __host__ __forceinline__ bool tag_normals(uint32_t t) { return (t >> 4) & 1u; }
+__device__ __host__ __forceinline__ int tag_material(uint32_t t) { return (int)(t >> 8); }
+
+// BVH2 node with both child boxes (64 B):
+//   f0 = (L.min.xyz, L.max.x) f1 = (L.max.yz, R.min.xy) f2 = (R.min.z, R.max.xyz)
+//   f3 = (left ref, right ref, split axis, 0) as int bits.
+// A child ref >= 0 is an interior node; a leaf ref has bit 31 set,
+// (count - 1) in bits 26-30 and the first primitive in bits 0-25.
+__device__ __host__ __forceinline__ bool ref_is_leaf(int r) { return r < 0; }
+__device__ __host__ __forceinline__ int leaf_first(int r) { return r & 0x03FFFFFF; }
+__device__ __host__ __forceinline__ int leaf_count(int r) { return ((r >> 26) & 31) + 1; }
+__host__ __forceinline__ int make_leaf_ref(int first, int count) {
+  return (int)(0x80000000u | ((uint32_t)(count - 1) << 26) | (uint32_t)first);
+}
+
+// Quantised node (48 B, 3 x 16 B loads): the union box's minimum corner and
+// per-axis power-of-two scales, then 8-bit child bounds rounded outward (min
+// down, max up) so the decoded box always contains the FP32 child box.
+//   f0 = (origin xyz, meta: exponent bytes x, y, z and the split axis)
+//   f1 = (L lo xyz + L hi x, L hi yz + R lo xy, R lo z + R hi xyz, left ref)
+//   f2 = (right ref, 0, 0, 0)
+struct QNode {
+  float ox, oy, oz;
+  uint32_t meta;
+  uint32_t lq0, lq1, rq;
+  int left;
+  int right;
+  int pad[3];
+};
+
+// Legacy material kinds of the reference shader (cuda_raytracer.cuh:43-55).
+enum Legacy : int {
+  L_LAMBERTIAN = 0, L_MIRROR = 1, L_GLASS = 2, L_LIGHT = 3, L_ROUGH_MIRROR = 4, L_CONSTANT = 5,
+  L_SHOW_NORMALS = 6, L_ANISO_METAL = 7, L_THIN_FILM = 8, L_CLEAR_COAT = 9, L_ABSORB = 15
+};
+
+// Material after the reference's apply_material mapping (cuda_raytracer.cuh:418-485):
+// kind, colour, roughness defaults and IOR rules resolved on the host.
+struct __align__(16) DevMaterial {
+  int kind;
+  int pattern;         // 0 none, 1 Fibonacci dots
+  float roughness;
+  float ior;           // per-material IOR (clear coat, thin film exterior)
+  f3 color;
+  float anisotropy;
+  f3 emission;
+  float film_thickness;
+  f3 eta;
+  float film_ior;
+  f3 k;
+  float pattern_p1;
+  f3 pattern_color;
+  float pattern_p2;
+};
+
+struct LightRec {      // one emitter sampled by next-event estimation
+  int prim;
+  float area;
+  float cdf;           // inclusive CDF over area
+  float pad;
+};
+
+struct SdfPrim {       // one SDF primitive (ray marched)
+  int type;
+  int material;
+  float px, py, pz;    // position
+  float a, b, c;       // parameters
+  float round;         // rounding radius (ROUND_BOX)
+  float r00, r01, r02, r10, r11, r12, r20, r21, r22;  // world->local rotation
+  float pad[2];
+};
+
+// Kernel-parameter view of a device scene (passed by value).
+struct SceneView {
+  const float4 *__restrict__ nodes;
+  const QNode *__restrict__ qnodes;
+  const float4 *__restrict__ prims;
+  const float4 *__restrict__ normals;  // 3 x float4 per primitive or null
+  const DevMaterial *__restrict__ mats;
+  const LightRec *__restrict__ lights;
+  const SdfPrim *__restrict__ sdf;
+  int root_ref;
+  int num_prims;
+  int num_mats;
+  int num_lights;
+  int use_bvh;
+  int quantized;
+  int num_sdf;
+  int sdf_steps;
+  float root_box[6];
+  float light_area;    // total emitter area
+  float sdf_k;         // smooth-union radius
+  float sdf_eps;
+  float pad_;
+};
+
+// Reference __constant__ settings (renderer_cuda_device.cu:18-26), passed by value.
+struct Globals {
+  float light_intensity;
+  float background_intensity;
+  float metal_fuzziness;
+  float glass_ior;
+  int dof_enabled;
+  float dof_aperture;
+  float dof_focus;
+  int nee;
+};
+
+// ---------------------------------------------------------------------------
+// Ray / box (hit_aabb, cuda_raytracer.cuh:154-197)
+// ---------------------------------------------------------------------------
+struct RayPre {
+  f3 o, d, inv;
+};
+__device__ __forceinline__ RayPre prep(const Ray &r) {
+  RayPre p;
+  p.o = r.o;
+  p.d = r.d;
+  p.inv = f3(1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z);
+  return p;
+}
+
+// Slab test. Swapping t0/t1 when inv < 0 is the same as taking the max bound as
+// the near plane, so the values compared are those of the reference.
+__device__ __forceinline__ bool box_hit(const RayPre &r, float x0, float y0, float z0, float x1, float y1,
+                                        float z1, float tmin, float tmax, float &tenter) {
+  float t0x = (x0 - r.o.x) * r.inv.x, t1x = (x1 - r.o.x) * r.inv.x;
+  if (r.inv.x < 0.0f) { float t = t0x; t0x = t1x; t1x = t; }
+  float t0y = (y0 - r.o.y) * r.inv.y, t1y = (y1 - r.o.y) * r.inv.y;
+  if (r.inv.y < 0.0f) { float t = t0y; t0y = t1y; t1y = t; }
+  float t0z = (z0 - r.o.z) * r.inv.z, t1z = (z1 - r.o.z) * r.inv.z;
+  if (r.inv.z < 0.0f) { float t = t0z; t0z = t1z; t1z = t; }
+  const float te = fmaxf(fmaxf(t0x, t0y), t0z);
+  const float tx = fminf(fminf(t1x, t1y), t1z);
+  tenter = te;
+  return te <= tx && tx >= tmin && te <= tmax;
+}
+
+// ---------------------------------------------------------------------------
+// Primitive tests returning only t (cuda_raytracer.cuh:203-347)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool t_sphere(const f3 &center, float radius, const Ray &r, float tmin, float tmax,
+                                         float &tout) {
+  f3 oc = r.o - center;
+  float a = dot(r.d, r.d);
+  float half_b = dot(oc, r.d);
+  float c = dot(oc, oc) - radius * radius;
+  float disc = half_b * half_b - a * c;
+  if (disc < 0) return false;
+  float sqrtd = sqrtf(disc);
+  float root = (-half_b - sqrtd) / a;
+  if (root < tmin || tmax < root) {
+    root = (-half_b + sqrtd) / a;
+    if (root < tmin || tmax < root) return false;
+  }
+  tout = root;
+  return true;
+}
+
+__device__ __forceinline__ bool t_rect(const f3 &corner, const f3 &u, const f3 &v, const Ray &r, float tmin,
+                                       float tmax, float &tout) {
+  f3 normal = normalize(f3(u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x));
+  float denom = dot(normal, r.d);
+  if (fabsf(denom) < 1e-8f) return false;
+  float t = dot(normal, corner - r.o) / denom;
+  if (t < tmin || t > tmax) return false;
+  f3 p = r.at(t) - corner;
+  float alpha = dot(p, u) / dot(u, u);
+  float beta = dot(p, v) / dot(v, v);
+  if (alpha < 0.0f || alpha > 1.0f || beta < 0.0f || beta > 1.0f) return false;
+  tout = t;
+  return true;
+}
+
+// Moller-Trumbore with the reference's comparisons; edges are stored
+// precomputed (e1 = v1 - v0, e2 = v2 - v0 in FP32, the values the reference
+// computes per test).
+__device__ __forceinline__ bool t_tri(const f3 &v0, const f3 &edge1, const f3 &edge2, const Ray &r, float tmin,
+                                      float tmax, float &tout) {
+  const f3 h = cross(r.d, edge2);
+  const float a = dot(edge1, h);
+  if (fabsf(a) < 1e-8f) return false;
+  const float f = 1.0f / a;
+  const f3 s = r.o - v0;
+  const float u = f * dot(s, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  const f3 q = cross(s, edge1);
+  const float v = f * dot(r.d, q);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  const float t = f * dot(edge2, q);
+  if (t < tmin || t > tmax) return false;
+  tout = t;
+  return true;
+}
+
+static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &r, float tmin, float tmax);
+
+__device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
+                                       float &t) {
+  const float4 *p = S.prims + 3 * (size_t)i;
+  const float4 a = __ldg(p);
+  const float4 c = __ldg(p + 2);
+  const uint32_t tag = __float_as_uint(c.w);
+  const uint32_t kind = tag_kind(tag);
+  if (kind == PK_SPHERE || kind == PK_DISPLACED) return t_sphere(f3(a.x, a.y, a.z), a.w, r, tmin, tmax, t);
+  const float4 b = __ldg(p + 1);
+  if (kind == PK_TRI)
+    return t_tri(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
+  if (kind == PK_RECT)
+    return t_rect(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
+  if (kind == PK_SDF) {
+    const float ts = sdf_march_prim(S, i, r, tmin, tmax);
+    if (ts >= 0.0f) { t = ts; return true; }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// Traversal (hit_scene, cuda_raytracer.cuh:487-602)
+// ---------------------------------------------------------------------------
+// The reference pops a node, tests its box against the current closest t and
+// pushes (far, near) by the sign of the ray on the node's split axis. Here the
+// parent holds both child boxes: each child is tested when its parent is
+// visited. The near child would be popped next in the reference with the same
+// closest t, so its result is identical. The far child is pushed with its
+// entry distance and re-checked against the closest t when popped; the other
+// two conditions of the slab test do not depend on the closest t and a child
+// rejected early would be rejected later as well (closest only shrinks). The
+// sequence of primitive tests, and so the closest-hit result with its
+// equal-t tie rule, is the reference's.
+//
+// Stack: the top RB_SHORT entries live in shared memory (one column per
+// thread, conflict-free), deeper ones in local memory. 32 entries in all; as
+// in the reference a push beyond 32 is dropped (and counted).
+#ifndef RB_SHORT
+#define RB_SHORT 8
+#endif
+#define RB_STACK 32
+
+struct Stack {
+  int2 *sh;     // shared column base for this thread; stride = blockDim
+  int stride;
+  int2 loc[RB_STACK - RB_SHORT];
+  int sp;
+  __device__ __forceinline__ void push(int ref, float te) {
+    const int2 e = make_int2(ref, __float_as_int(te));
+    if (sp < RB_SHORT) sh[sp * stride] = e;
+    else loc[sp - RB_SHORT] = e;
+    ++sp;
+  }
+  __device__ __forceinline__ int2 pop() {
+    --sp;
+    return sp < RB_SHORT ? sh[sp * stride] : loc[sp - RB_SHORT];
+  }
+};
+
+struct HitInfo {
+  float t;
+  int prim;
+};
+
+// Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
+template <bool ANY>
+__device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
+                                         uint32_t &overflow) {
+  HitInfo h;
+  h.t = tmax;
+  h.prim = -1;
+  float closest = tmax;
+  if (!S.use_bvh) {
+    for (int i = 0; i < S.num_prims; ++i) {
+      float t;
+      if (prim_t(S, i, ray, tmin, closest, t)) {
+        closest = t;
+        h.t = t;
+        h.prim = i;
+        if (ANY) return h;
+      }
+    }
+    return h;
+  }
+  const RayPre rp = prep(ray);
+  float te;
+  if (!box_hit(rp, S.root_box[0], S.root_box[1], S.root_box[2], S.root_box[3], S.root_box[4], S.root_box[5], tmin,
+               closest, te))
+    return h;
+  int cur = S.root_ref;
+  st.sp = 0;
+  while (true) {
+    if (ref_is_leaf(cur)) {
+      const int first = leaf_first(cur), cnt = leaf_count(cur);
+      for (int i = 0; i < cnt; ++i) {
+        float t;
+        if (prim_t(S, first + i, ray, tmin, closest, t)) {
+          closest = t;
+          h.t = t;
+          h.prim = first + i;
+          if (ANY) return h;
+        }
+      }
+    } else {
+      float tl, tr;
+      bool hl, hr;
+      int4 f3v;
+      if (!S.quantized) {
+        const float4 *n = S.nodes + 4 * (size_t)cur;
+        const float4 f0 = __ldg(n), f1 = __ldg(n + 1), f2 = __ldg(n + 2);
+        f3v = __ldg(reinterpret_cast<const int4 *>(n + 3));
+        hl = box_hit(rp, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, tmin, closest, tl);
+        hr = box_hit(rp, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, tmin, closest, tr);
+      } else {
+        const float4 *n = reinterpret_cast<const float4 *>(S.qnodes + cur);
+        const float4 q0 = __ldg(n);
+        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(n + 1));
+        const int rref = __ldg(reinterpret_cast<const int *>(n + 2));
+        const uint32_t meta = __float_as_uint(q0.w);
+        const float sx = __uint_as_float((meta & 0xFFu) << 23), sy = __uint_as_float(((meta >> 8) & 0xFFu) << 23),
+                    sz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
+#define RB_DQ(word, sh, o, s) fmaf((float)(((word) >> (sh)) & 0xFFu), (s), (o))
+        hl = box_hit(rp, RB_DQ(q1.x, 0, q0.x, sx), RB_DQ(q1.x, 8, q0.y, sy), RB_DQ(q1.x, 16, q0.z, sz),
+                     RB_DQ(q1.x, 24, q0.x, sx), RB_DQ(q1.y, 0, q0.y, sy), RB_DQ(q1.y, 8, q0.z, sz), tmin, closest, tl);
+        hr = box_hit(rp, RB_DQ(q1.y, 16, q0.x, sx), RB_DQ(q1.y, 24, q0.y, sy), RB_DQ(q1.z, 0, q0.z, sz),
+                     RB_DQ(q1.z, 8, q0.x, sx), RB_DQ(q1.z, 16, q0.y, sy), RB_DQ(q1.z, 24, q0.z, sz), tmin, closest, tr);
+#undef RB_DQ
+        f3v = make_int4((int)q1.w, rref, (int)(meta >> 24), 0);
+      }
+      const float dcomp = f3v.z == 0 ? ray.d.x : (f3v.z == 1 ? ray.d.y : ray.d.z);
+      const bool left_near = dcomp >= 0.0f;
+      const int nref = left_near ? f3v.x : f3v.y, fref = left_near ? f3v.y : f3v.x;
+      const bool hn = left_near ? hl : hr, hf = left_near ? hr : hl;
+      const float tf = left_near ? tr : tl;
+      if (hn) {
+        if (hf) {
+          if (st.sp < RB_STACK) st.push(fref, tf);
+          else ++overflow;
+        }
+        cur = nref;
+        continue;
+      }
+      if (hf) {
+        cur = fref;
+        continue;
+      }
+    }
+    // pop the next node whose entry distance still beats the closest hit
+    bool found = false;
+    while (st.sp > 0) {
+      const int2 e = st.pop();
+      if (__int_as_float(e.y) <= closest) {
+        cur = e.x;
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// Surface at the closest hit (hit record fields of cuda_raytracer.cuh:203-347)
+// ---------------------------------------------------------------------------
+struct Surface {
+  f3 p, n, tangent, center;
+  bool front;
+  bool visible;
+  int mat;
+};
+
+static __device__ Surface golf_surface(const f3 &center, float radius, const Ray &r, float t);
+static __device__ Surface sdf_surface(const SceneView &S, int prim, const Ray &r, float t);
+
+__device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, const HitInfo &h) {
+  const float4 *p = S.prims + 3 * (size_t)h.prim;
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  const uint32_t tag = __float_as_uint(c.w);
+  const uint32_t kind = tag_kind(tag);
+  Surface s;
+  s.visible = tag_visible(tag);
+  s.mat = tag_material(tag);
+  s.center = f3(0.0f, 0.0f, 0.0f);
+  if (kind == PK_SPHERE) {
+    const f3 center(a.x, a.y, a.z);
+    const float radius = a.w;
+    s.p = r.at(h.t);
+    f3 outward = (s.p - center) / radius;
+    s.front = dot(r.d, outward) < 0;
+    s.n = s.front ? outward : f3(-outward.x, -outward.y, -outward.z);
+    f3 tg = cross(f3(0.0f, 1.0f, 0.0f), outward);
+    if (tg.length_squared() < 1e-6f) tg = f3(1.0f, 0.0f, 0.0f);
+    s.tangent = normalize(tg);
+    s.center = center;
+  } else if (kind == PK_RECT) {
+    const f3 u(a.w, b.x, b.y), v(b.z, b.w, c.x);
+    f3 normal = normalize(f3(u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x));
+    s.p = r.at(h.t);
+    s.front = dot(r.d, normal) < 0;
+    s.n = s.front ? normal : f3(-normal.x, -normal.y, -normal.z);
+    s.tangent = normalize(u);
+  } else if (kind == PK_TRI) {
+    const f3 v0(a.x, a.y, a.z), e1(a.w, b.x, b.y), e2(b.z, b.w, c.x);
+    s.p = r.at(h.t);
+    const f3 geo = normalize(cross(e1, e2));
+    s.front = dot(r.d, geo) < 0;
+    f3 sn = geo;
+    const bool has_n = tag_normals(tag) && S.normals != nullptr;
+    if (has_n) {
+      const f3 hh = cross(r.d, e2);
+      const float f = 1.0f / dot(e1, hh);
+      const f3 sv = r.o - v0;
+      const float uu = f * dot(sv, hh);
+      const f3 q = cross(sv, e1);
+      const float vv = f * dot(r.d, q);
+      const float w = 1.0f - uu - vv;
+      const float4 *np = S.normals + 3 * (size_t)h.prim;
+      const f3 n0 = mk(__ldg(np)), n1 = mk(__ldg(np + 1)), n2 = mk(__ldg(np + 2));
+      sn = normalize(w * n0 + uu * n1 + vv * n2);
+      if (dot(sn, geo) < 0.0f) sn = -sn;
+    }
+    s.n = s.front ? sn : -sn;
+    if (has_n) {
+      const f3 incoming = -r.d;
+      if (dot(s.n, incoming) <= 0.0f) s.n = s.front ? geo : -geo;
+    }
+    s.tangent = normalize(e1);
+  } else if (kind == PK_DISPLACED) {
+    Surface g = golf_surface(f3(a.x, a.y, a.z), a.w, r, h.t);
+    g.visible = s.visible;
+    g.mat = s.mat;
+    return g;
+  } else {
+    Surface g = sdf_surface(S, h.prim, r, h.t);
+    g.visible = s.visible;
+    g.mat = s.mat;
+    return g;
+  }
+  return s;
+}
+
+}  // namespace rbd

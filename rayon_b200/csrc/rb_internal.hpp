@@ -1,0 +1,65 @@
+// Internal declarations shared by the translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rayon_b200.h"
+#include "rb_shade.cuh"
+
+namespace rb {
+
+inline float __int_as_float_host(int i) {
+  float f;
+  std::memcpy(&f, &i, 4);
+  return f;
+}
+inline float __uint_as_float_host(uint32_t i) {
+  float f;
+  std::memcpy(&f, &i, 4);
+  return f;
+}
+
+// Device layout assembled on the host before upload.
+struct HostLayout {
+  std::vector<float4> nodes;          // 4 per interior node
+  std::vector<rbd::QNode> qnodes;     // quantised copy of nodes
+  std::vector<float4> prims;          // 3 per primitive
+  std::vector<float4> normals;        // 3 per primitive (vertex normals) or empty
+  std::vector<rbd::DevMaterial> mats;
+  std::vector<rbd::LightRec> lights;
+  std::vector<rbd::SdfPrim> sdf;
+  int root_ref = 0;
+  float root_box[6] = {0, 0, 0, 0, 0, 0};
+  float light_area = 0.0f;
+  bool use_bvh = false;
+};
+
+struct DeviceScene {
+  rbd::SceneView view;
+  void *handle = nullptr;  // device pointer handed out as CudaScene::Scene*
+  size_t bytes = 0;
+};
+
+// FP32 camera frame for the kernels (cast from the FP64 frame, as
+// renderer_cuda_device.cu:279-284 casts its double arguments).
+struct FrameF {
+  rbd::f3 center, p00, du, dv, cu, cv;
+  int width, height, samples, sample_base, max_depth;
+  uint32_t seed, salt;
+  int min_adaptive;
+  float adaptive_threshold;
+};
+
+bool cuda_ok(cudaError_t e, const char *what);
+void set_error(const std::string &msg);
+DeviceScene *lookup_scene(const void *handle);
+void build_quantized(HostLayout &L);
+FrameF frame_from(const double *fr, int w, int h);
+rbd::Globals current_globals();
+rb_render_opts current_opts();
+
+}  // namespace rb

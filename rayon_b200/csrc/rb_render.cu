@@ -1,0 +1,995 @@
+// Device scene upload, the per-frame render kernels and the drop-in C-ABI
+// (renderer_cuda_device.cuh:8-67) of the B200 render path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "host_scene.hpp"
+#include "rb_internal.hpp"
+#include "rb_shade.cuh"
+
+using namespace rbd;
+
+namespace rb {
+
+const HostScene &host_scene_of(const rb_scene_desc *s);
+
+std::atomic<unsigned long long> g_launches{0};
+
+// ---------------------------------------------------------------------------
+// Registries (host side)
+// ---------------------------------------------------------------------------
+static std::mutex g_mu;
+static std::unordered_map<const void *, DeviceScene *> g_scenes;   // handle -> scene
+static std::unordered_map<const void *, size_t> g_accum_bytes;      // accum allocations
+static std::unordered_map<const void *, uint32_t> g_rng_ctx;        // samples already drawn
+
+bool cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+DeviceScene *lookup_scene(const void *handle) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_scenes.find(handle);
+  return it == g_scenes.end() ? nullptr : it->second;
+}
+
+// Reference __constant__ defaults (renderer_cuda_device.cu:18-26).
+static Globals g_globals = {1.0f, 1.0f, 0.8f, 1.5f, 0, 0.1f, 10.0f, 0};
+static rb_render_opts g_opts = {0, 1, 0x5EEDu, 16, 16, {0, 0, 0, 0}};
+Globals current_globals() {
+  Globals g = g_globals;
+  g.nee = g_opts.nee;
+  return g;
+}
+rb_render_opts current_opts() { return g_opts; }
+
+// ---------------------------------------------------------------------------
+// Host -> device layout
+// ---------------------------------------------------------------------------
+static float ftz_sub(float a, float b) {
+  float r = a - b;
+  if (std::fabs(r) < 1.17549435e-38f) r = std::copysign(0.0f, r);
+  return r;
+}
+
+static DevMaterial resolve_material(const rb_material_desc &d) {
+  // apply_material (cuda_raytracer.cuh:418-485), resolved once per material.
+  DevMaterial m;
+  std::memset(&m, 0, sizeof m);
+  auto f = [](const double *v) { return f3((float)v[0], (float)v[1], (float)v[2]); };
+  const f3 albedo = f(d.albedo);
+  m.color = albedo;
+  m.emission = f(d.emission);
+  m.eta = f(d.eta);
+  m.k = f(d.k);
+  m.roughness = d.roughness;
+  m.ior = d.refractive_index;
+  m.anisotropy = d.anisotropy;
+  m.film_thickness = d.film_thickness;
+  m.film_ior = d.film_ior;
+  m.pattern = d.pattern == 1 ? 1 : 0;  // FIBONACCI_DOTS; other patterns fall to the base colour
+  m.pattern_color = f(d.pattern_color);
+  m.pattern_p1 = d.pattern_param1;
+  m.pattern_p2 = d.pattern_param2;
+  switch (d.type) {
+    case RB_MAT_LAMBERTIAN: m.kind = L_LAMBERTIAN; break;
+    case RB_MAT_MIRROR: m.kind = L_MIRROR; break;
+    case RB_MAT_METAL:
+    case RB_MAT_ROUGH_MIRROR:
+      m.kind = L_ROUGH_MIRROR;
+      m.roughness = d.roughness > 0.0f ? d.roughness : 0.3f;
+      break;
+    case RB_MAT_GLASS:
+    case RB_MAT_DIELECTRIC: m.kind = L_GLASS; break;
+    case RB_MAT_LIGHT: m.kind = L_LIGHT; break;
+    case RB_MAT_CONSTANT: m.kind = L_CONSTANT; break;
+    case RB_MAT_SHOW_NORMALS: m.kind = L_SHOW_NORMALS; break;
+    case RB_MAT_ANISOTROPIC_METAL: m.kind = L_ANISO_METAL; break;
+    case RB_MAT_SDF_MATERIAL: m.kind = L_LAMBERTIAN; break;
+    case RB_MAT_THIN_FILM: m.kind = L_THIN_FILM; break;
+    case RB_MAT_CLEAR_COAT:
+      m.kind = L_CLEAR_COAT;
+      m.ior = d.refractive_index > 1.0f ? d.refractive_index : 1.5f;
+      break;
+    default: m.kind = L_ABSORB; break;
+  }
+  return m;
+}
+
+static void put(float4 *r, int w, float v) { reinterpret_cast<float *>(r)[w] = v; }
+static float getw(const float4 *r, int w) { return reinterpret_cast<const float *>(r)[w]; }
+
+// Rotation (radians, X then Y then Z) to a world->local matrix.
+static void rot_matrix(const double r[3], float out[9]) {
+  const double cx = std::cos(r[0]), sx = std::sin(r[0]);
+  const double cy = std::cos(r[1]), sy = std::sin(r[1]);
+  const double cz = std::cos(r[2]), sz = std::sin(r[2]);
+  // local->world R = Rz * Ry * Rx; world->local = R^T
+  const double R[3][3] = {
+      {cz * cy, cz * sy * sx - sz * cx, cz * sy * cx + sz * sx},
+      {sz * cy, sz * sy * sx + cz * cx, sz * sy * cx - cz * sx},
+      {-sy, cy * sx, cy * cx}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out[3 * i + j] = (float)R[j][i];
+}
+
+static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts, HostLayout &L) {
+  const size_t n = hs.geoms.size();
+  L.prims.assign(3 * n, make_float4(0, 0, 0, 0));
+  L.mats.resize(hs.materials.size());
+  for (size_t i = 0; i < hs.materials.size(); ++i) L.mats[i] = resolve_material(hs.materials[i]);
+  bool any_normals = false;
+  for (const auto &g : hs.geoms) any_normals |= (g.type == RB_GEOM_TRIANGLE && g.has_normals);
+  if (any_normals) L.normals.assign(3 * n, make_float4(0, 0, 0, 0));
+  L.sdf.clear();
+  double light_area = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    const Geom &g = hs.geoms[i];
+    float4 *r = &L.prims[3 * i];
+    uint32_t kind = PK_NONE;
+    const float *pf = nullptr;
+    (void)pf;
+    switch (g.type) {
+      case RB_GEOM_SPHERE:
+      case RB_GEOM_DISPLACED_SPHERE:
+        kind = g.type == RB_GEOM_SPHERE ? PK_SPHERE : PK_DISPLACED;
+        for (int k = 0; k < 4; ++k) put(r, k, (float)g.p[k]);
+        break;
+      case RB_GEOM_RECTANGLE:
+        kind = PK_RECT;
+        for (int k = 0; k < 9; ++k) put(r, k, (float)g.p[k]);
+        break;
+      case RB_GEOM_TRIANGLE: {
+        kind = PK_TRI;
+        float v[9];
+        for (int k = 0; k < 9; ++k) v[k] = (float)g.p[k];
+        for (int k = 0; k < 3; ++k) {
+          put(r, k, v[k]);
+          put(r, 3 + k, ftz_sub(v[3 + k], v[k]));
+          put(r, 6 + k, ftz_sub(v[6 + k], v[k]));
+        }
+        if (g.has_normals && any_normals)
+          for (int k = 0; k < 3; ++k)
+            L.normals[3 * i + k] = make_float4((float)g.p[9 + 3 * k], (float)g.p[10 + 3 * k], (float)g.p[11 + 3 * k], 0.0f);
+        break;
+      }
+      case RB_GEOM_SDF_PRIMITIVE: {
+        kind = PK_SDF;
+        SdfPrim q;
+        std::memset(&q, 0, sizeof q);
+        const int t = (int)g.p[0];
+        q.type = (t == RB_SDF_ROUND_BOX) ? 32 : t;
+        q.material = g.material_id;
+        q.px = (float)g.p[1]; q.py = (float)g.p[2]; q.pz = (float)g.p[3];
+        q.a = (float)g.p[4]; q.b = (float)g.p[5]; q.c = (float)g.p[6];
+        double bound = 0.0;
+        if (t == RB_SDF_SPHERE) bound = g.p[4];
+        else if (t == RB_SDF_BOX) bound = std::sqrt(g.p[4] * g.p[4] + g.p[5] * g.p[5] + g.p[6] * g.p[6]);
+        else if (t == RB_SDF_ROUND_BOX) {
+          // rounded box: half extents in params, rounding radius = min half extent * 0.2
+          bound = std::sqrt(g.p[4] * g.p[4] + g.p[5] * g.p[5] + g.p[6] * g.p[6]);
+          q.round = (float)(0.2 * std::min(g.p[4], std::min(g.p[5], g.p[6])));
+        } else if (t == RB_SDF_TORUS) bound = g.p[4] + g.p[5];
+        else if (t == RB_SDF_CAPSULE) bound = g.p[4] + 0.5 * g.p[5];
+        else { kind = PK_NONE; break; }
+        float R[9];
+        const double rr[3] = {g.p[7], g.p[8], g.p[9]};
+        rot_matrix(rr, R);
+        q.r00 = R[0]; q.r01 = R[1]; q.r02 = R[2]; q.r10 = R[3]; q.r11 = R[4]; q.r12 = R[5];
+        q.r20 = R[6]; q.r21 = R[7]; q.r22 = R[8];
+        const double pad = hs.sdf.blend_k + 1e-3;
+        put(r, 0, q.px); put(r, 1, q.py); put(r, 2, q.pz); put(r, 3, (float)(bound * 1.0001 + pad));
+        put(r, 4, __int_as_float_host((int)L.sdf.size()));
+        L.sdf.push_back(q);
+        break;
+      }
+      default:
+        kind = PK_NONE;  // CUBE / TRIANGLE_MESH are not converted (scene_builder_cuda.cu:138-140)
+        break;
+    }
+    uint32_t mat = (g.material_id >= 0 && g.material_id < (int)hs.materials.size()) ? (uint32_t)g.material_id : 0xFFFFFFu;
+    const uint32_t tag = kind | ((uint32_t)(g.visible ? 1 : 0) << 3) |
+                         ((uint32_t)((g.has_normals && any_normals) ? 1 : 0) << 4) | (mat << 8);
+    put(r, 11, __uint_as_float_host(tag));
+    // emitters for next-event estimation
+    if (mat != 0xFFFFFFu && L.mats[mat].kind == L_LIGHT &&
+        (kind == PK_RECT || kind == PK_TRI || kind == PK_SPHERE)) {
+      const DevMaterial &m = L.mats[mat];
+      if (m.emission.x > 0 || m.emission.y > 0 || m.emission.z > 0) {
+        double area = 0.0;
+        if (kind == PK_SPHERE) area = 4.0 * M_PI * (double)getw(r, 3) * (double)getw(r, 3);
+        else {
+          const double ax = getw(r, 3), ay = getw(r, 4), az = getw(r, 5);
+          const double bx = getw(r, 6), by = getw(r, 7), bz = getw(r, 8);
+          const double cx = ay * bz - az * by, cy = az * bx - ax * bz, cz = ax * by - ay * bx;
+          area = std::sqrt(cx * cx + cy * cy + cz * cz) * (kind == PK_TRI ? 0.5 : 1.0);
+        }
+        if (area > 0) {
+          light_area += area;
+          LightRec lr;
+          lr.prim = (int)i;
+          lr.area = (float)area;
+          lr.cdf = (float)light_area;
+          lr.pad = 0;
+          L.lights.push_back(lr);
+        }
+      }
+    }
+  }
+  L.light_area = (float)light_area;
+  if (!L.lights.empty()) L.lights.back().cdf = 3.0e38f;  // the last bin takes any rounding excess
+
+  // BVH: interior nodes only, each holding its two children's boxes.
+  L.use_bvh = hs.use_bvh && opts.use_bvh && !hs.nodes.empty() && hs.root >= 0;
+  L.nodes.clear();
+  L.root_ref = 0;
+  for (int k = 0; k < 6; ++k) L.root_box[k] = 0.0f;
+  if (L.use_bvh) {
+    std::vector<int> remap(hs.nodes.size(), -1);
+    int m = 0;
+    for (size_t i = 0; i < hs.nodes.size(); ++i)
+      if (!hs.nodes[i].is_leaf) remap[i] = m++;
+    auto ref_of = [&](int i) -> int {
+      const Node &c = hs.nodes[i];
+      if (c.is_leaf) return make_leaf_ref(c.a, std::max(1, c.b));
+      return remap[i];
+    };
+    for (size_t i = 0; i < hs.nodes.size(); ++i) {
+      const Node &nd = hs.nodes[i];
+      if (nd.is_leaf) {
+        if (nd.a >= (1 << 26) || nd.b > 32) { set_error("BVH leaf beyond the device encoding"); return false; }
+        continue;
+      }
+      const Node &l = hs.nodes[nd.a], &rr = hs.nodes[nd.b];
+      float4 q[4];
+      float *w = reinterpret_cast<float *>(q);
+      for (int k = 0; k < 3; ++k) { w[k] = (float)l.bmin[k]; w[3 + k] = (float)l.bmax[k]; }
+      for (int k = 0; k < 3; ++k) { w[6 + k] = (float)rr.bmin[k]; w[9 + k] = (float)rr.bmax[k]; }
+      int *wi = reinterpret_cast<int *>(&q[3]);
+      wi[0] = ref_of(nd.a);
+      wi[1] = ref_of(nd.b);
+      wi[2] = nd.split_axis;
+      wi[3] = 0;
+      for (int k = 0; k < 4; ++k) L.nodes.push_back(q[k]);
+    }
+    const Node &root = hs.nodes[hs.root];
+    for (int k = 0; k < 3; ++k) { L.root_box[k] = (float)root.bmin[k]; L.root_box[3 + k] = (float)root.bmax[k]; }
+    L.root_ref = ref_of(hs.root);
+    if (opts.quantized_bvh) build_quantized(L);
+  }
+  return true;
+}
+
+template <typename T>
+static bool upload_vec(const std::vector<T> &v, T **dst, cudaStream_t st, size_t &bytes) {
+  *dst = nullptr;
+  if (v.empty()) return true;
+  const size_t nb = v.size() * sizeof(T);
+  if (!cuda_ok(cudaMalloc((void **)dst, nb), "cudaMalloc(scene)")) return false;
+  bytes += nb;
+  return cuda_ok(cudaMemcpyAsync(*dst, v.data(), nb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(scene)");
+}
+
+void free_device_scene(DeviceScene *ds) {
+  if (!ds) return;
+  cudaFree((void *)ds->view.nodes);
+  cudaFree((void *)ds->view.qnodes);
+  cudaFree((void *)ds->view.prims);
+  cudaFree((void *)ds->view.normals);
+  cudaFree((void *)ds->view.mats);
+  cudaFree((void *)ds->view.lights);
+  cudaFree((void *)ds->view.sdf);
+  cudaFree(ds->handle);
+  delete ds;
+}
+
+DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaStream_t st) {
+  HostLayout L;
+  if (!build_device_layout(hs, opts, L)) return nullptr;
+  DeviceScene *ds = new DeviceScene();
+  std::memset(&ds->view, 0, sizeof ds->view);
+  SceneView &v = ds->view;
+  size_t bytes = 0;
+  float4 *nodes = nullptr, *prims = nullptr, *normals = nullptr;
+  QNode *qn = nullptr;
+  DevMaterial *mats = nullptr;
+  LightRec *lights = nullptr;
+  SdfPrim *sdf = nullptr;
+  bool ok = upload_vec(L.nodes, &nodes, st, bytes) && upload_vec(L.qnodes, &qn, st, bytes) &&
+            upload_vec(L.prims, &prims, st, bytes) && upload_vec(L.normals, &normals, st, bytes) &&
+            upload_vec(L.mats, &mats, st, bytes) && upload_vec(L.lights, &lights, st, bytes) &&
+            upload_vec(L.sdf, &sdf, st, bytes);
+  v.nodes = nodes; v.qnodes = qn; v.prims = prims; v.normals = normals; v.mats = mats;
+  v.lights = lights; v.sdf = sdf;
+  v.root_ref = L.root_ref;
+  v.num_prims = (int)hs.geoms.size();
+  v.num_mats = (int)hs.materials.size();
+  v.num_lights = (int)L.lights.size();
+  v.use_bvh = L.use_bvh ? 1 : 0;
+  v.quantized = (L.use_bvh && opts.quantized_bvh) ? 1 : 0;
+  v.num_sdf = (int)L.sdf.size();
+  v.sdf_steps = hs.sdf.max_steps;
+  v.sdf_eps = hs.sdf.epsilon;
+  v.sdf_k = hs.sdf.blend_k;
+  for (int k = 0; k < 6; ++k) v.root_box[k] = L.root_box[k];
+  v.light_area = L.light_area;
+  // The handle is a small device allocation so that it is a genuine device
+  // pointer, as CudaScene::Scene* is in the reference (scene_builder_cuda.cu:294-296).
+  ok = ok && cuda_ok(cudaMalloc(&ds->handle, 256), "cudaMalloc(scene handle)") &&
+       cuda_ok(cudaMemcpyAsync(ds->handle, &v, sizeof v, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(handle)") &&
+       cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize(upload)");
+  ds->bytes = bytes + 256;
+  if (!ok) {
+    free_device_scene(ds);
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_scenes[ds->handle] = ds;
+  return ds;
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void kahan_add(float &sum, float &c, float x) {
+  const float y = __fsub_rn(x, c);
+  const float t = __fadd_rn(sum, y);
+  c = __fsub_rn(__fsub_rn(t, sum), y);
+  sum = t;
+}
+
+// Primary hits through pixel centres (offsets 0 in render_acc_kernel.cu:200-214).
+__global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t *ids, float *tout) {
+  extern __shared__ int2 smem[];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  if (x >= P.width || y >= P.height) return;
+  Stack st;
+  st.sh = smem + tid;
+  st.stride = blockDim.x * blockDim.y;
+  uint32_t ovf = 0;
+  const f3 pc = P.p00 + ((float)x + 0.0f) * P.du + ((float)y + 0.0f) * P.dv;
+  Ray r;
+  r.o = P.center;
+  r.d = pc - P.center;
+  const HitInfo h = trace<false>(S, r, 0.001f, FLT_MAX, st, ovf);
+  const int pix = y * P.width + x;
+  ids[pix] = h.prim;
+  if (tout) tout[pix] = h.prim >= 0 ? h.t : -1.0f;
+}
+
+// Camera ray of one sample (render_acc_kernel.cu:198-222); lens by polar mapping.
+__device__ __forceinline__ Ray camera_ray(const FrameF &P, const Globals &G, int x, int y, uint32_t key) {
+  const float ou = rb_draw(key, RB_DIM_JITTER) - 0.5f;
+  const float ov = rb_draw(key, RB_DIM_JITTER + 1) - 0.5f;
+  const f3 pc = P.p00 + ((float)x + ou) * P.du + ((float)y + ov) * P.dv;
+  Ray r;
+  r.o = P.center;
+  r.d = pc - P.center;
+  if (G.dof_enabled && G.dof_aperture > 0.0f) {
+    const f3 nd = normalize(r.d);
+    const f3 focus = P.center + G.dof_focus * nd;
+    const float rr = sqrtf(rb_draw(key, RB_DIM_LENS));
+    float s, c;
+    __sincosf(2.0f * RB_PI * rb_draw(key, RB_DIM_LENS + 1), &s, &c);
+    const f3 off = G.dof_aperture * ((rr * c) * P.cu + (rr * s) * P.cv);
+    r.o = P.center + off;
+    r.d = focus - r.o;
+  }
+  return r;
+}
+
+// One path segment: trace, shade, NEE, Russian roulette. Returns true when the
+// path ended (radiance complete in L).
+template <bool NEE>
+__device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &G, Stack &st, uint32_t &ovf, Ray &ray,
+                                             f3 &thr, f3 &L, int &bounce, float &prev_pdf, uint32_t key,
+                                             int max_depth) {
+  const HitInfo h = trace<false>(S, ray, 0.001f, FLT_MAX, st, ovf);
+  if (h.prim < 0) {
+    if (G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * G.background_intensity;
+    return true;
+  }
+  const Surface sf = surface(S, ray, h);
+  if (!sf.visible && bounce == 0) {  // camera rays pass through invisible geometry
+    ray.o = sf.p + ray.d * 0.01f;
+    return ++bounce >= max_depth;
+  }
+  if (sf.mat >= S.num_mats) return true;
+  const DevMaterial &m = S.mats[sf.mat];
+  const ScatterOut so = scatter(G, m, sf, ray, key, bounce);
+  if (so.emit.length_squared() > 0.0f) {
+    float w = 1.0f;
+    if (NEE && prev_pdf > 0.0f && m.kind == L_LIGHT && S.num_lights > 0) {
+      // MIS weight of the BSDF strategy for an emitter that NEE also samples
+      const float dl = h.t * ray.d.length();
+      const f3 ud = normalize(ray.d);
+      f3 gn = sf.n;  // |cos| at the light only needs the line, not the side
+      const float cl = fabsf(dot(gn, ud));
+      const float pl = cl > 0.0f ? dl * dl / (cl * S.light_area) : 0.0f;
+      w = mis2(prev_pdf, pl);
+    }
+    L = L + thr * so.emit * w;
+  }
+  if (!so.scattered) return true;
+  if (NEE) {
+    prev_pdf = 0.0f;
+    if (m.kind == L_LAMBERTIAN && bounce + 1 < max_depth && S.num_lights > 0) {
+      LightSample ls;
+      const uint32_t dl = rb_vdim(bounce, RB_SLOT_LIGHT);
+      if (sample_light(S, G, rb_draw(key, dl), rb_draw(key, dl + 1), rb_draw(key, dl + 2), ls)) {
+        const f3 o = so.ray.o;
+        const f3 dv = ls.p - o;
+        const float d2 = dv.length_squared();
+        const float dist = sqrtf(d2);
+        const f3 wi = dv / dist;
+        const f3 nn = normalize(sf.n);
+        const float cs = dot(nn, wi);
+        const float cl = fabsf(dot(ls.n, wi));
+        if (cs > 0.0f && cl > 0.0f) {
+          Ray sr;
+          sr.o = o;
+          sr.d = wi;
+          const HitInfo sh = trace<true>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
+          if (sh.prim < 0) {
+            const float pl = d2 / (cl * S.light_area);
+            const float pb = cs * (1.0f / RB_PI);
+            const float w = mis2(pl, pb);
+            // f * Le * cos / pdf_l with f = albedo / pi; the albedo is the scatter attenuation
+            L = L + thr * so.att * ls.Le * (cs * (1.0f / RB_PI) * w / pl);
+          }
+        }
+      }
+      prev_pdf = so.pdf;
+    }
+  }
+  thr = thr * so.att;
+  if (bounce > 0) {
+    const float mc = fmaxf(thr.x, fmaxf(thr.y, thr.z));
+    const float sp = fminf(mc, 0.95f);
+    if (rb_draw(key, rb_vdim(bounce, RB_SLOT_RR)) > sp) return true;
+    thr = thr / sp;
+  }
+  ray = so.ray;
+  return ++bounce >= max_depth;
+}
+
+// Per-pixel progressive kernel: one thread owns one pixel for the launch and
+// runs its samples back to back in a single flattened loop (one path segment
+// per iteration), so a lane whose path ended starts its next sample at once
+// instead of idling until the warp's longest path finishes.
+template <bool NEE>
+__global__ void __launch_bounds__(256) k_render(SceneView S, Globals G, FrameF P, float4 *__restrict__ acc,
+                                                float4 *__restrict__ comp, int *__restrict__ counts,
+                                                unsigned long long *__restrict__ counters) {
+  extern __shared__ int2 smem[];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const bool inside = x < P.width && y < P.height;
+  const int pix = inside ? y * P.width + x : 0;
+  int have = 0;
+  bool work = inside;
+  if (work && counts) {
+    have = counts[pix];
+    if (have < 0) work = false;  // converged (sign bit, render_acc_kernel.cu:165-170)
+  }
+  unsigned long long segs = 0;
+  if (work) {
+    Stack st;
+    st.sh = smem + tid;
+    st.stride = blockDim.x * blockDim.y;
+    uint32_t ovf = 0;
+    const float4 a0 = acc[pix];
+    float sx = a0.x, sy = a0.y, sz = a0.z;
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    if (comp) {
+      const float4 c0 = comp[pix];
+      cx = c0.x; cy = c0.y; cz = c0.z;
+    }
+    float lum_before = 0.0f;
+    if (counts && have > 0) {
+      const float inv = 1.0f / (float)have;
+      lum_before = 0.299f * sx * inv + 0.587f * sy * inv + 0.114f * sz * inv;
+    }
+    int s = 0, bounce = 0;
+    bool alive = false;
+    Ray ray;
+    f3 thr(1.f, 1.f, 1.f), L(0.f, 0.f, 0.f);
+    uint32_t key = 0;
+    float prev_pdf = 0.0f;
+    while (true) {
+      if (!alive) {
+        if (s >= P.samples) break;
+        key = rb_path_key(P.seed, P.salt, (uint32_t)pix, (uint32_t)(P.sample_base + s));
+        ++s;
+        ray = camera_ray(P, G, x, y, key);
+        thr = f3(1.f, 1.f, 1.f);
+        L = f3(0.f, 0.f, 0.f);
+        bounce = 0;
+        prev_pdf = 0.0f;
+        alive = true;
+      }
+      ++segs;
+      if (path_segment<NEE>(S, G, st, ovf, ray, thr, L, bounce, prev_pdf, key, P.max_depth)) {
+        if (comp) {
+          kahan_add(sx, cx, L.x);
+          kahan_add(sy, cy, L.y);
+          kahan_add(sz, cz, L.z);
+        } else {
+          sx += L.x; sy += L.y; sz += L.z;
+        }
+        alive = false;
+      }
+    }
+    acc[pix] = make_float4(sx, sy, sz, 0.0f);
+    if (comp) comp[pix] = make_float4(cx, cy, cz, 0.0f);
+    if (counts) {  // convergence test (render_acc_kernel.cu:241-271)
+      const int nc = have + P.samples;
+      if (nc >= P.min_adaptive) {
+        const float inv = 1.0f / (float)nc;
+        const float lum_after = 0.299f * sx * inv + 0.587f * sy * inv + 0.114f * sz * inv;
+        const float rel = fabsf(lum_after - lum_before) / fmaxf(lum_after, 0.001f);
+        counts[pix] = rel < P.adaptive_threshold ? -nc : nc;
+      } else {
+        counts[pix] = nc;
+      }
+    }
+    if (counters && ovf) atomicAdd(counters + 2, (unsigned long long)ovf);
+  }
+  if (counters) {
+    // warp-aggregated segment and path counts
+    unsigned long long paths = work ? (unsigned long long)P.samples : 0ull;
+    for (int o = 16; o > 0; o >>= 1) {
+      segs += __shfl_down_sync(0xffffffffu, segs, o);
+      paths += __shfl_down_sync(0xffffffffu, paths, o);
+    }
+    if ((tid & 31) == 0) {
+      atomicAdd(counters, segs);
+      atomicAdd(counters + 1, paths);
+    }
+  }
+}
+
+// accum float4 sums -> u8 (gammaCorrectKernel, render_acc_kernel.cu:11-44)
+__global__ void k_gamma(const float4 *__restrict__ acc, unsigned char *__restrict__ out, int w, int h, int spp,
+                        int ch, float gamma, const int *__restrict__ counts) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const int pix = y * w + x;
+  const float4 a = acc[pix];
+  int n = counts ? abs(counts[pix]) : spp;
+  if (n <= 0) n = 1;
+  const float inv = 1.0f / (float)n, ig = 1.0f / gamma;
+  const float r = fminf(powf(fmaxf(a.x * inv, 0.0f), ig), 0.999f);
+  const float g = fminf(powf(fmaxf(a.y * inv, 0.0f), ig), 0.999f);
+  const float b = fminf(powf(fmaxf(a.z * inv, 0.0f), ig), 0.999f);
+  unsigned char *o = out + (size_t)pix * ch;
+  o[0] = (unsigned char)(256.0f * r);
+  o[1] = (unsigned char)(256.0f * g);
+  o[2] = (unsigned char)(256.0f * b);
+  if (ch == 4) o[3] = 255;
+}
+
+// Plasma colour ramp, 8 control points (the sample heat map's table,
+// render_acc_kernel.cu:50-82).
+__constant__ float c_plasma[8][4] = {
+    {0.000f, 0.050f, 0.030f, 0.530f}, {0.143f, 0.230f, 0.015f, 0.660f}, {0.286f, 0.450f, 0.005f, 0.660f},
+    {0.429f, 0.650f, 0.060f, 0.540f}, {0.571f, 0.820f, 0.170f, 0.360f}, {0.714f, 0.940f, 0.340f, 0.170f},
+    {0.857f, 0.990f, 0.560f, 0.040f}, {1.000f, 0.940f, 0.975f, 0.130f}};
+
+__global__ void k_heatmap(const int *__restrict__ counts, unsigned char *__restrict__ out, int w, int h, int ch,
+                          int max_s) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const int pix = y * w + x;
+  const int c = abs(counts[pix]);
+  float t = max_s > 0 ? fminf((float)c / (float)max_s, 1.0f) : 0.0f;
+  t = fminf(fmaxf(t, 0.0f), 1.0f);
+  float r = c_plasma[7][1], g = c_plasma[7][2], b = c_plasma[7][3];
+  for (int i = 0; i < 7; ++i) {
+    if (t <= c_plasma[i + 1][0]) {
+      const float lt = (t - c_plasma[i][0]) / (c_plasma[i + 1][0] - c_plasma[i][0]);
+      r = c_plasma[i][1] + lt * (c_plasma[i + 1][1] - c_plasma[i][1]);
+      g = c_plasma[i][2] + lt * (c_plasma[i + 1][2] - c_plasma[i][2]);
+      b = c_plasma[i][3] + lt * (c_plasma[i + 1][3] - c_plasma[i][3]);
+      break;
+    }
+  }
+  unsigned char *o = out + (size_t)pix * ch;
+  o[0] = (unsigned char)(255.0f * r);
+  o[1] = (unsigned char)(255.0f * g);
+  o[2] = (unsigned char)(255.0f * b);
+  if (ch == 4) o[3] = 255;
+}
+
+__global__ void k_count_negative(const int *__restrict__ counts, int n, int *__restrict__ out) {
+  int local = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) local += counts[i] < 0;
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
+__global__ void k_f3_to_f4(const float *__restrict__ in, float4 *__restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
+}
+__global__ void k_f4_to_f3(const float4 *__restrict__ in, float *__restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const float4 v = in[i];
+    out[3 * i] = v.x;
+    out[3 * i + 1] = v.y;
+    out[3 * i + 2] = v.z;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+// ---------------------------------------------------------------------------
+FrameF frame_from(const double *fr, int w, int h) {
+  FrameF P;
+  std::memset(&P, 0, sizeof P);
+  auto g = [&](int i) { return f3((float)fr[3 * i], (float)fr[3 * i + 1], (float)fr[3 * i + 2]); };
+  P.center = g(0);
+  P.p00 = g(1);
+  P.du = g(2);
+  P.dv = g(3);
+  P.cu = g(4);
+  P.cv = g(5);
+  P.width = w;
+  P.height = h;
+  return P;
+}
+
+int launch_primary(const DeviceScene *ds, const FrameF &P, int32_t *ids, float *t, cudaStream_t st) {
+  dim3 blk(16, 16), grd((P.width + 15) / 16, (P.height + 15) / 16);
+  const size_t sm = sizeof(int2) * RB_SHORT * blk.x * blk.y;
+  k_primary<<<grd, blk, sm, st>>>(ds->view, P, ids, t);
+  g_launches++;
+  return cuda_ok(cudaGetLastError(), "k_primary launch") ? RB_OK : RB_ERR_CUDA;
+}
+
+int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, int *counts,
+                  unsigned long long *counters, cudaStream_t st) {
+  const rb_render_opts o = current_opts();
+  int bx = o.block_x > 0 ? o.block_x : 16, by = o.block_y > 0 ? o.block_y : 16;
+  if (bx * by > 256) { bx = 16; by = 16; }
+  dim3 blk(bx, by), grd((P.width + bx - 1) / bx, (P.height + by - 1) / by);
+  const size_t sm = sizeof(int2) * RB_SHORT * blk.x * blk.y;
+  if (G.nee)
+    k_render<true><<<grd, blk, sm, st>>>(ds->view, G, P, acc, comp, counts, counters);
+  else
+    k_render<false><<<grd, blk, sm, st>>>(ds->view, G, P, acc, comp, counts, counters);
+  g_launches++;
+  return cuda_ok(cudaGetLastError(), "k_render launch") ? RB_OK : RB_ERR_CUDA;
+}
+
+// Display stream and pinned staging (renderer_cuda_device.cu:31-54).
+static cudaStream_t s_display = nullptr;
+static unsigned char *s_pinned = nullptr;
+static size_t s_pinned_size = 0;
+static unsigned char *s_dev_display = nullptr;
+static size_t s_dev_display_size = 0;
+
+static bool ensure_display(size_t bytes) {
+  if (!s_dev_display || s_dev_display_size != bytes) {
+    if (s_dev_display) cudaFree(s_dev_display);
+    s_dev_display = nullptr;
+    if (!cuda_ok(cudaMalloc(&s_dev_display, bytes), "cudaMalloc(display)")) return false;
+    s_dev_display_size = bytes;
+  }
+  if (s_display && (!s_pinned || s_pinned_size != bytes)) {
+    if (s_pinned) cudaFreeHost(s_pinned);
+    s_pinned = nullptr;
+    if (!cuda_ok(cudaMallocHost(&s_pinned, bytes), "cudaMallocHost(display)")) return false;
+    s_pinned_size = bytes;
+  }
+  return true;
+}
+
+static void finish_display(unsigned char *out, size_t bytes) {
+  if (s_display && s_pinned) {
+    cudaMemcpyAsync(s_pinned, s_dev_display, bytes, cudaMemcpyDeviceToHost, s_display);
+    cudaStreamSynchronize(s_display);
+    std::memcpy(out, s_pinned, bytes);
+  } else {
+    cudaDeviceSynchronize();
+    cudaMemcpy(out, s_dev_display, bytes, cudaMemcpyDeviceToHost);
+  }
+}
+
+}  // namespace rb
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+using namespace rb;
+
+extern "C" {
+
+void initCudaStreams(void) {
+  if (!s_display) cuda_ok(cudaStreamCreateWithFlags(&s_display, cudaStreamNonBlocking), "initCudaStreams");
+}
+
+void cleanupCudaStreams(void) {
+  if (s_display) {
+    cudaStreamDestroy(s_display);
+    s_display = nullptr;
+  }
+  if (s_pinned) {
+    cudaFreeHost(s_pinned);
+    s_pinned = nullptr;
+    s_pinned_size = 0;
+  }
+}
+
+void setLightIntensity(float v) { g_globals.light_intensity = v; }
+void setBackgroundIntensity(float v) { g_globals.background_intensity = v; }
+void setMetalFuzziness(float v) { g_globals.metal_fuzziness = v; }
+void setGlassRefractionIndex(float v) { g_globals.glass_ior = v; }
+void setDOFEnabled(bool e) { g_globals.dof_enabled = e ? 1 : 0; }
+void setDOFAperture(float v) { g_globals.dof_aperture = v; }
+void setDOFFocusDistance(float v) { g_globals.dof_focus = v; }
+
+void rb_get_render_opts(rb_render_opts *o) {
+  if (o) *o = g_opts;
+}
+void rb_set_render_opts(const rb_render_opts *o) {
+  if (o) g_opts = *o;
+}
+
+void freeDeviceRandomStates(void *p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_rng_ctx.erase(p);
+  }
+  cudaFree(p);
+}
+
+void freeDeviceAccumBuffer(void *p) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_accum_bytes.erase(p);
+  }
+  cudaFree(p);
+}
+
+void resetDeviceAccumBuffer(void *p, int num_pixels) {
+  if (!p || num_pixels <= 0) return;
+  size_t bytes = (size_t)num_pixels * sizeof(float4);
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_accum_bytes.find(p);
+    if (it != g_accum_bytes.end()) bytes = std::min(it->second, 2 * bytes);  // sums and compensation
+  }
+  cuda_ok(cudaMemset(p, 0, bytes), "resetDeviceAccumBuffer");
+}
+
+unsigned long long renderPixelsCUDAAccumulative(
+    unsigned char *image, float *accum_buffer, rb_cuda_scene *scene, int width, int height, double ccx,
+    double ccy, double ccz, double p0x, double p0y, double p0z, double dux, double duy, double duz, double dvx,
+    double dvy, double dvz, int samples_to_add, int total_samples_so_far, int max_depth, void **d_rand_states_ptr,
+    void **d_accum_buffer_ptr, double cux, double cuy, double cuz, double cvx, double cvy, double cvz,
+    void *d_pixel_sample_counts, int min_adaptive_samples, float adaptive_threshold) {
+  (void)image;
+  (void)total_samples_so_far;
+  if (!scene) return 0ull;
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("renderPixelsCUDAAccumulative: scene handle was not created by this library");
+    return 0ull;
+  }
+  if (width <= 0 || height <= 0 || samples_to_add < 0 || !d_rand_states_ptr || !d_accum_buffer_ptr) {
+    set_error("renderPixelsCUDAAccumulative: invalid argument");
+    return 0ull;
+  }
+  const int n = width * height;
+  cudaStream_t st = 0;
+  // RNG context: the per-path streams are counter based; the context keeps
+  // the index of the next sample so that successive calls draw new samples.
+  if (*d_rand_states_ptr == nullptr) {
+    void *p = nullptr;
+    if (!cuda_ok(cudaMalloc(&p, 256), "cudaMalloc(rng context)")) return 0ull;
+    *d_rand_states_ptr = p;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_rng_ctx[p] = 0;
+  }
+  float4 *acc = nullptr;
+  const size_t nb = (size_t)n * sizeof(float4);
+  if (*d_accum_buffer_ptr == nullptr) {
+    if (!cuda_ok(cudaMalloc((void **)&acc, 2 * nb), "cudaMalloc(accum)")) return 0ull;
+    *d_accum_buffer_ptr = acc;
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      g_accum_bytes[acc] = 2 * nb;
+    }
+    cudaMemsetAsync(acc, 0, 2 * nb, st);
+    if (accum_buffer) {
+      float *tmp = nullptr;
+      if (!cuda_ok(cudaMalloc(&tmp, (size_t)n * 12), "cudaMalloc(accum staging)")) return 0ull;
+      cudaMemcpyAsync(tmp, accum_buffer, (size_t)n * 12, cudaMemcpyHostToDevice, st);
+      k_f3_to_f4<<<(n + 255) / 256, 256, 0, st>>>(tmp, acc, n);
+      g_launches++;
+      cudaStreamSynchronize(st);
+      cudaFree(tmp);
+    }
+  } else {
+    acc = static_cast<float4 *>(*d_accum_buffer_ptr);
+  }
+  float4 *comp = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_accum_bytes.find(acc);
+    if (it != g_accum_bytes.end() && it->second >= 2 * nb) comp = acc + n;
+  }
+  uint32_t base = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_rng_ctx.find(*d_rand_states_ptr);
+    if (it != g_rng_ctx.end()) {
+      base = it->second;
+      it->second += (uint32_t)samples_to_add;
+    }
+  }
+  const double fr[21] = {ccx, ccy, ccz, p0x, p0y, p0z, dux, duy, duz, dvx, dvy, dvz, cux, cuy, cuz, cvx, cvy, cvz, 0, 0, 0};
+  FrameF P = frame_from(fr, width, height);
+  P.samples = samples_to_add;
+  P.sample_base = (int)base;
+  P.max_depth = max_depth;
+  P.seed = current_opts().seed;
+  P.salt = 0;
+  P.min_adaptive = min_adaptive_samples;
+  P.adaptive_threshold = adaptive_threshold;
+  const rb_render_opts o = current_opts();
+  if (samples_to_add > 0)
+    launch_render(ds, current_globals(), P, acc, o.kahan ? comp : nullptr, static_cast<int *>(d_pixel_sample_counts),
+                  nullptr, st);
+  cuda_ok(cudaStreamSynchronize(st), "renderPixelsCUDAAccumulative");
+  if (accum_buffer) {
+    float *tmp = nullptr;
+    if (cuda_ok(cudaMalloc(&tmp, (size_t)n * 12), "cudaMalloc(accum staging)")) {
+      k_f4_to_f3<<<(n + 255) / 256, 256, 0, st>>>(acc, tmp, n);
+      g_launches++;
+      cuda_ok(cudaMemcpy(accum_buffer, tmp, (size_t)n * 12, cudaMemcpyDeviceToHost), "accum download");
+      cudaFree(tmp);
+    }
+  }
+  return (unsigned long long)n * (unsigned long long)samples_to_add;
+}
+
+void convertAccumToDisplayCUDA(void *d_acc, unsigned char *img, int w, int h, int ch, int spp, float gamma,
+                               void *counts) {
+  if (!d_acc || !img || spp <= 0) return;
+  const size_t bytes = (size_t)w * h * ch;
+  if (!ensure_display(bytes)) return;
+  dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
+  cudaStream_t st = s_display ? s_display : 0;
+  k_gamma<<<grd, blk, 0, st>>>(static_cast<const float4 *>(d_acc), s_dev_display, w, h, spp, ch, gamma,
+                                static_cast<const int *>(counts));
+  g_launches++;
+  finish_display(img, bytes);
+}
+
+void allocateAdaptiveBuffer(void **p, int n) {
+  if (!p || *p) return;
+  if (cuda_ok(cudaMalloc(p, (size_t)n * sizeof(int)), "allocateAdaptiveBuffer"))
+    cudaMemset(*p, 0, (size_t)n * sizeof(int));
+}
+void resetAdaptiveBuffer(void *p, int n) {
+  if (p) cudaMemset(p, 0, (size_t)n * sizeof(int));
+}
+void freeAdaptiveBuffer(void *p) {
+  if (p) cudaFree(p);
+}
+
+int countConvergedPixels(void *p, int n) {
+  if (!p || n <= 0) return 0;
+  int *d = nullptr;
+  if (!cuda_ok(cudaMalloc(&d, sizeof(int)), "countConvergedPixels")) return 0;
+  cudaMemset(d, 0, sizeof(int));
+  k_count_negative<<<std::min(1184, (n + 255) / 256), 256>>>(static_cast<const int *>(p), n, d);
+  g_launches++;
+  int out = 0;
+  cudaMemcpy(&out, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return out;
+}
+
+void renderSampleHeatmapCUDA(void *counts, unsigned char *img, int w, int h, int ch, int max_s) {
+  if (!counts || !img) return;
+  const size_t bytes = (size_t)w * h * ch;
+  if (!ensure_display(bytes)) return;
+  dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
+  k_heatmap<<<grd, blk, 0, s_display ? s_display : 0>>>(static_cast<const int *>(counts), s_dev_display, w, h, ch,
+                                                          max_s);
+  g_launches++;
+  finish_display(img, bytes);
+}
+
+rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opts, void *stream) {
+  if (!s) {
+    set_error("rb_scene_upload: null scene");
+    return nullptr;
+  }
+  rb_upload_opts o;
+  std::memset(&o, 0, sizeof o);
+  o.use_bvh = 1;
+  if (opts) o = *opts;
+  DeviceScene *ds = upload_scene(host_scene_of(s), o, static_cast<cudaStream_t>(stream));
+  return ds ? static_cast<rb_cuda_scene *>(ds->handle) : nullptr;
+}
+
+void rb_scene_free_device(rb_cuda_scene *scene) {
+  if (!scene) return;
+  DeviceScene *ds = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_scenes.find(scene);
+    if (it == g_scenes.end()) return;
+    ds = it->second;
+    g_scenes.erase(it);
+  }
+  cudaDeviceSynchronize();
+  free_device_scene(ds);
+}
+
+int64_t rb_scene_device_bytes(const rb_cuda_scene *scene) {
+  DeviceScene *ds = lookup_scene(scene);
+  return ds ? (int64_t)ds->bytes : 0;
+}
+
+int rb_primary_hits(const rb_cuda_scene *scene, int w, int h, const double frame[21], int32_t *ids, float *t,
+                    void *stream) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_primary_hits: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  if (w <= 0 || h <= 0 || !frame || !ids) {
+    set_error("rb_primary_hits: invalid argument");
+    return RB_ERR_INVALID_ARG;
+  }
+  return launch_primary(ds, frame_from(frame, w, h), ids, t, static_cast<cudaStream_t>(stream));
+}
+
+int rb_render_accumulate(const rb_cuda_scene *scene, int w, int h, const double frame[21], int samples,
+                         int sample_base, int max_depth, float *accum, float *comp, uint64_t *counters,
+                         void *stream) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_render_accumulate: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  if (w <= 0 || h <= 0 || !frame || !accum || samples < 0 || max_depth < 0 || sample_base < 0) {
+    set_error("rb_render_accumulate: invalid argument");
+    return RB_ERR_INVALID_ARG;
+  }
+  if (samples == 0) return RB_OK;
+  FrameF P = frame_from(frame, w, h);
+  P.samples = samples;
+  P.sample_base = sample_base;
+  P.max_depth = max_depth;
+  P.seed = current_opts().seed;
+  P.salt = 0;
+  return launch_render(ds, current_globals(), P, reinterpret_cast<float4 *>(accum), reinterpret_cast<float4 *>(comp),
+                       nullptr, reinterpret_cast<unsigned long long *>(counters), static_cast<cudaStream_t>(stream));
+}
+
+unsigned long long rb_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"
