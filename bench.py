@@ -1,0 +1,346 @@
+"""Benchmark of the B200 render path (one JSON line on rank 0).
+
+Workload: the Cornell box (512x512, 256 spp, max depth 16, FP32 radiance with
+Kahan-compensated accumulation, background 0). One step = one full frame:
+512*512*256 = 67.1 M primary paths. `value` = Mpaths/s with the scene and the
+accumulation buffers resident in HBM (device time, CUDA events per step on the
+launching stream, L2 flushed between steps). `e2e` = the same frames through
+the drop-in C-ABI call exactly as RayON's offline renderer makes it
+(renderer_cuda_host.hpp:23-74): scene upload from host memory, five
+renderPixelsCUDAAccumulative calls with a host float3 accumulation buffer
+(uploaded on the first call, downloaded after every call), free.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU renderer (RendererCPUParallel,
+compiled from the reference sources into oracle/_ref/) on the host cores on a
+bounded sample of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(name="cornell", width=512, height=512, spp=256, depth=16)
+METRIC = "Mpaths/s (Cornell box 512x512, 256 spp, depth 16)"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the render kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "k_render_cornell.txt"
+    if f.exists():
+        for line in f.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                try:
+                    return float(line.split(":")[1])
+                except ValueError:
+                    return None
+    return None
+
+
+def cpu_reference_sample(spec, budget_s: float = 12.0):
+    """RendererCPUParallel (reference sources, oracle/_ref) on a bounded sample."""
+    from oracle import refbind
+    if not refbind.host_available():
+        return None
+    r = refbind.RefScene(spec)
+    w, h = spec.width, spec.height
+    secs, _, threads, rays = r.render_cpu_parallel(spec.camera, w, h, 1)
+    spp = max(1, min(spec.spp, int(budget_s / max(secs, 1e-3))))
+    if spp > 1:
+        secs, _, threads, rays = r.render_cpu_parallel(spec.camera, w, h, spp)
+    paths = w * h * spp
+    return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+            "sample": f"RendererCPUParallel on the {w}x{h} frame at {spp} spp ({paths} paths, {secs:.1f} s; "
+                      f"FP64, linear scan, depth 16, non-Lambert materials as Lambert)",
+            "seconds": secs, "paths": paths}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from rayon_b200 import scenes
+    spec = scenes.cornell(**{k: WORKLOAD[k] for k in ("width", "height", "spp", "depth")})
+    from oracle import refbind
+    if not refbind.host_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference drivers (oracle/_ref) not built"}))
+        return
+    r = refbind.RefScene(spec)
+    w, h = spec.width, spec.height
+    # bounded sample per step: spp chosen so one step is ~5 s of host work
+    secs1, _, threads, _ = r.render_cpu_parallel(spec.camera, w, h, 1)
+    spp = max(1, min(spec.spp, int(5.0 / max(secs1, 1e-3))))
+    for _ in range(args.warmup):
+        r.render_cpu_parallel(spec.camera, w, h, 1)
+    times = []
+    for _ in range(args.steps):
+        s, _, threads, _ = r.render_cpu_parallel(spec.camera, w, h, spp)
+        times.append(s)
+    paths = w * h * spp
+    t = sum(times) / len(times)
+    v = paths / t / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cornell {w}x{h}, {spp} spp per step (of 256), depth 16 fixed by the renderer",
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+                         "sample": f"{w}x{h} at {spp} spp per step, RendererCPUParallel"},
+        "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rayon_b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from rayon_b200 import lib, render, scenes
+    spec = scenes.cornell(**{k: WORKLOAD[k] for k in ("width", "height", "spp", "depth")})
+    w, h, spp, depth = spec.width, spec.height, spec.spp, spec.depth
+    paths = w * h * spp
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = np.ascontiguousarray(spec.camera.frame(w, h), np.float64)
+    frp = fr.ctypes.data_as(C.POINTER(C.c_double))
+    render.set_globals(background=spec.background)
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    acc = torch.zeros((w * h, 4), dtype=torch.float32, device="cuda")
+    comp = torch.zeros_like(acc)
+    counters = torch.zeros(4, dtype=torch.int64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
+
+    def step(i, cnt=None):
+        st = lib.rb_render_accumulate(ds.handle, w, h, frp, spp, (rank * 1000003 + i) * spp % (1 << 30), depth,
+                                      C.c_void_p(acc.data_ptr()), C.c_void_p(comp.data_ptr()),
+                                      C.c_void_p(cnt.data_ptr()) if cnt is not None else None, sptr)
+        if st != 0:
+            raise RuntimeError(render.lib.rb_last_error().decode())
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    # segment / path counts of one frame (for Mrays/s and the work-based roofline)
+    counters.zero_()
+    step(0, counters)
+    torch.cuda.synchronize()
+    segs, npaths, overflow = [int(x) for x in counters[:3].cpu()]
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.rb_launch_count()
+    evs = []
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step(args.warmup + i)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+    launches = lib.rb_launch_count() - launches0
+    ms = [a.elapsed_time(b) for a, b in evs]
+    t_ms = sum(ms) / len(ms)
+    if world > 1:
+        tt = torch.tensor([t_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(tt.item())
+        torch.distributed.barrier()
+    value = world * paths / (t_ms * 1e-3) / 1e6
+
+    # ---- e2e: the drop-in call with host buffers, as the reference's offline renderer
+    e2e = None
+    h2d = d2h = 0
+    if True:
+        torch.cuda.synchronize()
+        e2e_times = []
+        for i in range(max(1, min(3, args.steps))):
+            t0 = time.perf_counter()
+            ds2 = sc.upload()
+            img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
+            ds2.free()
+            torch.cuda.synchronize()
+            e2e_times.append(time.perf_counter() - t0)
+            h2d = ds.nbytes + w * h * 12
+            d2h = 5 * w * h * 12
+        e2e_t = min(e2e_times) if world == 1 else max(e2e_times)
+        e2e = {"value": world * paths / e2e_t / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_t,
+               "path": "renderPixelsCUDAAccumulative x5 + scene upload (host float3 accumulation)"}
+        mean_rad = float(img.reshape(-1, 3).mean() / spp)
+
+    peaks, peaks_kind = measured_peaks()
+    # roofline of the render kernel: its DRAM-bound bytes are the accumulation
+    # state (sum + Kahan compensation, read and written: 64 B per pixel); the
+    # scene (~2 KB) lives in L1. The kernel is bound by instruction issue, so
+    # the issue roof is reported beside it from counted work.
+    alg_bytes = w * h * 64
+    achieved = alg_bytes / (t_ms * 1e-3) / 1e9
+    sm_mhz = None
+    res = {
+        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"cornell {w}x{h}, {spp} spp, depth {depth}, 30 primitives, background 0",
+                   "paths_per_step": paths, "kernel": "k_render (per-pixel, flattened sample x bounce loop)",
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "mrays_per_s": world * segs / (t_ms * 1e-3) / 1e6,
+        "segments_per_path": segs / max(npaths, 1),
+        "stack_overflows": overflow,
+        "gpu_launches": int(launches),
+        "e2e": e2e,
+    }
+    clocks = clk.summary()
+    res["clocks"] = clocks
+    sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                       "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(),
+                       "peak_kind": f"{peaks_kind} HBM copy bandwidth",
+                       "algorithmic_bytes_per_launch": alg_bytes}
+    if rank == 0 and world == 1 and not args.no_reference_cuda:
+        res["reference_cuda"] = reference_cuda(spec, fr)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            res["cpu_baseline"] = cpu_reference_sample(spec)
+        except Exception as e:  # noqa: BLE001
+            res["cpu_baseline"] = {"unavailable": str(e)}
+    res["fp32_issue_peak_tflops_at_clock"] = fp32_peak
+    res["mean_radiance"] = mean_rad
+    if rank == 0:
+        print(json.dumps(res))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def reference_cuda(spec, fr):
+    """The reference's own CUDA renderer (renderAccKernel via its
+    renderPixelsCUDAAccumulative, compiled for sm_100a from its sources) on
+    the same frame, device-resident call timed with CUDA events."""
+    from oracle import refbind
+    if not refbind.cuda_available():
+        return {"unavailable": "oracle/_ref/librayon_ref_cuda.so not built"}
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    import make_golden as mg
+    L, MD = mg._cuda_lib()
+    sh = mg.ref_cuda_scene(L, MD, spec)
+    L.refc_set_globals(1.0, spec.background, 0.8, 1.5, 0, 0.1, 10.0)
+    w, h = spec.width, spec.height
+    frp = fr.ctypes.data_as(C.POINTER(C.c_double))
+    L.refc_render_device(sh, w, h, frp, 16, spec.depth, None)  # warm-up
+    ms = [L.refc_render_device(sh, w, h, frp, spec.spp, spec.depth, None) for _ in range(3)]
+    secs = L.refc_render(sh, w, h, frp, spec.spp, 5, spec.depth, None)
+    L.refc_scene_destroy(sh)
+    best = min(ms)
+    paths = w * h * spec.spp
+    return {"mpaths_s": paths / (best * 1e-3) / 1e6, "ms_per_frame": best,
+            "e2e_mpaths_s": paths / secs / 1e6 if secs > 0 else None,
+            "note": "reference renderAccKernel (sm_100a build of its sources, -maxrregcount 80, fast math)"}
+
+
+if __name__ == "__main__":
+    main()

@@ -19,7 +19,7 @@
 #include <cstring>
 #include <thread>
 
-#include "rayon_b200.h"
+#include "rayon_b200_scene.h"
 #include "render/renderer_interface.hpp"
 #include "renderer_cpu_parallel.hpp"
 #include "scene_description.hpp"

@@ -508,9 +508,10 @@ __global__ void __launch_bounds__(256) k_render(SceneView S, Globals G, FrameF P
     f3 thr(1.f, 1.f, 1.f), L(0.f, 0.f, 0.f);
     uint32_t key = 0;
     float prev_pdf = 0.0f;
+    const int nsamples = P.max_depth > 0 ? P.samples : 0;  // depth 0: no bounce, black (ray_color's empty loop)
     while (true) {
       if (!alive) {
-        if (s >= P.samples) break;
+        if (s >= nsamples) break;
         key = rb_path_key(P.seed, P.salt, (uint32_t)pix, (uint32_t)(P.sample_base + s));
         ++s;
         ray = camera_ray(P, G, x, y, key);

@@ -126,7 +126,7 @@ __device__ __forceinline__ f3 fib_point(int i, int n) {
 }
 static __device__ __noinline__ f3 fib_dots(const DevMaterial &m, const f3 &base, const f3 &p, const f3 &c) {
   const f3 q = normalize(normalize(p - c));
-  const int n = (int)m.pattern_p1;
+  const int n = min(max((int)m.pattern_p1, 0), 4096);
   float best = -1.0f;
   for (int i = 0; i < n; ++i) best = fmaxf(best, dot(q, fib_point(i, n)));
   best = fmaxf(fminf(best, 1.0f), -1.0f);

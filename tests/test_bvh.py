@@ -1,0 +1,87 @@
+"""BVH build parity: the native builder against the reference's own buildBVH
+(golden fixtures from tests/golden/make_golden.py --bvh, and live when the
+reference drivers are built)."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+from cases import BVH_CASES  # noqa: E402
+
+from rayon_b200 import scene as S  # noqa: E402
+from rayon_b200 import scenes  # noqa: E402
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _same(e, g, order):
+    assert e.root == int(g["root"])
+    np.testing.assert_array_equal(e.bounds, g["bounds"])  # exact FP64
+    np.testing.assert_array_equal(e.a, g["a"])
+    np.testing.assert_array_equal(e.b, g["b"])
+    np.testing.assert_array_equal(e.is_leaf, g["is_leaf"])
+    np.testing.assert_array_equal(e.split_axis, g["split_axis"])
+    np.testing.assert_array_equal(order, g["order"])
+
+
+@pytest.mark.parametrize("name", sorted(BVH_CASES))
+@pytest.mark.parametrize("threads", [1, 0])
+def test_bvh_matches_reference_golden(name, threads):
+    spec = BVH_CASES[name]()
+    sc = spec.to_scene()
+    sc.build_bvh(threads=threads)
+    g = np.load(GOLDEN / f"bvh_{name}.npz")
+    _same(sc.export_bvh(), g, sc.export_order())
+
+
+def test_bvh_live_reference_random_scene():
+    from oracle import refbind
+    if not refbind.host_available():
+        pytest.skip("reference drivers not built (no reference tree here)")
+    rng = np.random.default_rng(123)
+    n = 6000
+    k = rng.integers(0, 3, n).astype(np.uint8)
+    p = np.zeros((n, 18))
+    p[:, :9] = rng.normal(size=(n, 9)) * 10
+    p[k == 0, 3] = rng.uniform(0.1, 2, (k == 0).sum())
+    m = np.zeros(n, np.int32)
+    spec = scenes.SceneSpec("rand", [S.lambertian((0.5, 0.5, 0.5))], k, p, m, scenes.Camera((0, 0, -40), (0, 0, 0)),
+                            32, 32, 1, 2)
+    r = refbind.RefScene(spec)
+    r.build_bvh()
+    g = r.export()
+    sc = spec.to_scene()
+    sc.build_bvh()
+    _same(sc.export_bvh(), g, sc.export_order())
+
+
+def test_empty_and_single():
+    sc = S.SceneDescription()
+    sc.add_material(S.lambertian((1, 1, 1)))
+    sc.build_bvh()
+    assert sc.export_bvh().root == -1
+    sc.add_sphere((0, 0, 0), 1.0, 0)
+    sc.build_bvh()
+    e = sc.export_bvh()
+    assert e.root == 0 and e.is_leaf[0] == 1 and e.b[0] == 1
+
+
+@pytest.mark.parametrize("leaf", [1, 2, 8, 16])
+def test_leaf_size_variants_are_valid_trees(leaf):
+    spec = BVH_CASES["small_icospheres"]()
+    sc = spec.to_scene()
+    sc.build_bvh(max_leaf=leaf)
+    e = sc.export_bvh()
+    g = sc.export_geometry()
+    seen = np.zeros(g.shape[0], int)
+    for i in np.nonzero(e.is_leaf)[0]:
+        assert 1 <= e.b[i] <= leaf
+        seen[e.a[i]:e.a[i] + e.b[i]] += 1
+        lo, hi = e.bounds[i, :3], e.bounds[i, 3:]
+        assert (g[e.a[i]:e.a[i] + e.b[i], 22:25] >= lo).all() and (g[e.a[i]:e.a[i] + e.b[i], 25:28] <= hi).all()
+    assert (seen == 1).all()
+    for i in np.nonzero(e.is_leaf == 0)[0]:
+        for c in (e.a[i], e.b[i]):
+            assert (e.bounds[c, :3] >= e.bounds[i, :3]).all() and (e.bounds[c, 3:] <= e.bounds[i, 3:]).all()
