@@ -219,8 +219,9 @@ typedef struct rb_render_opts {
   int nee;            /* 1: next-event estimation with MIS on area lights   */
   int kahan;          /* 1: Kahan-compensated FP32 accumulation (default 1) */
   uint32_t seed;      /* RNG seed of the per-path counter-based streams     */
-  int block_x, block_y; /* launch shape of the per-pixel kernel (0 = tuned) */
-  int reserved[4];
+  int block_x, block_y; /* launch shape of the per-pixel kernel (0 = tuned per class) */
+  int reserved[4];      /* [0]: resident 256-thread blocks per SM the kernel is
+                           compiled for (1-4; 0 = tuned per material class) */
 } rb_render_opts;
 void rb_get_render_opts(rb_render_opts *out);
 void rb_set_render_opts(const rb_render_opts *in);

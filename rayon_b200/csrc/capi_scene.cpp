@@ -118,8 +118,21 @@ int64_t rb_scene_add_triangles(rb_scene_desc *s, const double *v, const double *
 }
 
 int rb_scene_set_visible(rb_scene_desc *s, int64_t i, int visible) {
-  if (!s || i < 0 || i >= (int64_t)s->s.geoms.size()) return RB_ERR_INVALID_ARG;
-  s->s.geoms[i].visible = visible ? 1 : 0;
+  // i is the insertion index (the index an add call returned), also after a
+  // BVH build has permuted the geometries to leaf order.
+  if (!s || i < 0 || i >= (int64_t)s->s.geoms.size()) {
+    rb::set_error("rb_scene_set_visible: geometry index out of range");
+    return RB_ERR_INVALID_ARG;
+  }
+  auto &g = s->s.geoms;
+  if (g[i].orig != i) {
+    for (auto &q : g)
+      if (q.orig == i) {
+        q.visible = visible ? 1 : 0;
+        return RB_OK;
+      }
+  }
+  g[i].visible = visible ? 1 : 0;
   return RB_OK;
 }
 

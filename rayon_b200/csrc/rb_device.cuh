@@ -256,6 +256,7 @@ __device__ __forceinline__ bool t_tri(const f3 &v0, const f3 &edge1, const f3 &e
 
 static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &r, float tmin, float tmax);
 
+template <int MS>
 __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
                                        float &t) {
   const float4 *p = S.prims + 3 * (size_t)i;
@@ -269,7 +270,7 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
     return t_tri(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
   if (kind == PK_RECT)
     return t_rect(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
-  if (kind == PK_SDF) {
+  if (MS >= 3 && kind == PK_SDF) {
     const float ts = sdf_march_prim(S, i, r, tmin, tmax);
     if (ts >= 0.0f) { t = ts; return true; }
   }
@@ -321,7 +322,7 @@ struct HitInfo {
 };
 
 // Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
-template <bool ANY>
+template <bool ANY, int MS>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {
   HitInfo h;
@@ -331,7 +332,7 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
   if (!S.use_bvh) {
     for (int i = 0; i < S.num_prims; ++i) {
       float t;
-      if (prim_t(S, i, ray, tmin, closest, t)) {
+      if (prim_t<MS>(S, i, ray, tmin, closest, t)) {
         closest = t;
         h.t = t;
         h.prim = i;
@@ -352,7 +353,7 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
       const int first = leaf_first(cur), cnt = leaf_count(cur);
       for (int i = 0; i < cnt; ++i) {
         float t;
-        if (prim_t(S, first + i, ray, tmin, closest, t)) {
+        if (prim_t<MS>(S, first + i, ray, tmin, closest, t)) {
           closest = t;
           h.t = t;
           h.prim = first + i;
@@ -431,6 +432,7 @@ struct Surface {
 static __device__ Surface golf_surface(const f3 &center, float radius, const Ray &r, float t);
 static __device__ Surface sdf_surface(const SceneView &S, int prim, const Ray &r, float t);
 
+template <int MS>
 __device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, const HitInfo &h) {
   const float4 *p = S.prims + 3 * (size_t)h.prim;
   const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
@@ -484,12 +486,12 @@ __device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, con
       if (dot(s.n, incoming) <= 0.0f) s.n = s.front ? geo : -geo;
     }
     s.tangent = normalize(e1);
-  } else if (kind == PK_DISPLACED) {
+  } else if (MS >= 3 && kind == PK_DISPLACED) {
     Surface g = golf_surface(f3(a.x, a.y, a.z), a.w, r, h.t);
     g.visible = s.visible;
     g.mat = s.mat;
     return g;
-  } else {
+  } else if (MS >= 3) {
     Surface g = sdf_surface(S, h.prim, r, h.t);
     g.visible = s.visible;
     g.mat = s.mat;

@@ -36,12 +36,14 @@ struct HostLayout {
   float root_box[6] = {0, 0, 0, 0, 0, 0};
   float light_area = 0.0f;
   bool use_bvh = false;
+  int ms = 3;  // kernel material class
 };
 
 struct DeviceScene {
   rbd::SceneView view;
   void *handle = nullptr;  // device pointer handed out as CudaScene::Scene*
   size_t bytes = 0;
+  int ms = 3;
 };
 
 // FP32 camera frame for the kernels (cast from the FP64 frame, as

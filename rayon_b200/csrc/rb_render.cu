@@ -44,7 +44,7 @@ DeviceScene *lookup_scene(const void *handle) {
 
 // Reference __constant__ defaults (renderer_cuda_device.cu:18-26).
 static Globals g_globals = {1.0f, 1.0f, 0.8f, 1.5f, 0, 0.1f, 10.0f, 0};
-static rb_render_opts g_opts = {0, 1, 0x5EEDu, 16, 16, {0, 0, 0, 0}};
+static rb_render_opts g_opts = {0, 1, 0x5EEDu, 0, 0, {0, 0, 0, 0}};
 Globals current_globals() {
   Globals g = g_globals;
   g.nee = g_opts.nee;
@@ -226,6 +226,14 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     }
   }
   L.light_area = (float)light_area;
+  // smallest kernel class covering the scene (materials and primitive kinds)
+  L.ms = RB_MS_DIFFUSE;
+  for (const auto &m : L.mats) {
+    if (m.kind == L_MIRROR || m.kind == L_ROUGH_MIRROR || m.kind == L_GLASS) L.ms = std::max(L.ms, RB_MS_CLASSIC);
+    if (m.kind == L_ANISO_METAL || m.kind == L_THIN_FILM || m.kind == L_CLEAR_COAT || m.pattern) L.ms = RB_MS_FULL;
+  }
+  for (const auto &g : hs.geoms)
+    if (g.type == RB_GEOM_DISPLACED_SPHERE || g.type == RB_GEOM_SDF_PRIMITIVE) L.ms = RB_MS_FULL;
   if (!L.lights.empty()) L.lights.back().cdf = 3.0e38f;  // the last bin takes any rounding excess
 
   // BVH: interior nodes only, each holding its two children's boxes.
@@ -264,7 +272,10 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     const Node &root = hs.nodes[hs.root];
     for (int k = 0; k < 3; ++k) { L.root_box[k] = (float)root.bmin[k]; L.root_box[3 + k] = (float)root.bmax[k]; }
     L.root_ref = ref_of(hs.root);
-    if (opts.quantized_bvh) build_quantized(L);
+    if (opts.quantized_bvh) {
+      build_quantized(L);
+      L.nodes.clear();  // the quantised copy replaces the FP32 nodes on the device
+    }
   }
   return true;
 }
@@ -328,6 +339,7 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
        cuda_ok(cudaMemcpyAsync(ds->handle, &v, sizeof v, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(handle)") &&
        cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize(upload)");
   ds->bytes = bytes + 256;
+  ds->ms = L.ms;
   if (!ok) {
     free_device_scene(ds);
     return nullptr;
@@ -362,7 +374,7 @@ __global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t 
   Ray r;
   r.o = P.center;
   r.d = pc - P.center;
-  const HitInfo h = trace<false>(S, r, 0.001f, FLT_MAX, st, ovf);
+  const HitInfo h = trace<false, RB_MS_FULL>(S, r, 0.001f, FLT_MAX, st, ovf);
   const int pix = y * P.width + x;
   ids[pix] = h.prim;
   if (tout) tout[pix] = h.prim >= 0 ? h.t : -1.0f;
@@ -391,23 +403,23 @@ __device__ __forceinline__ Ray camera_ray(const FrameF &P, const Globals &G, int
 
 // One path segment: trace, shade, NEE, Russian roulette. Returns true when the
 // path ended (radiance complete in L).
-template <bool NEE>
+template <bool NEE, int MS>
 __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &G, Stack &st, uint32_t &ovf, Ray &ray,
                                              f3 &thr, f3 &L, int &bounce, float &prev_pdf, uint32_t key,
                                              int max_depth) {
-  const HitInfo h = trace<false>(S, ray, 0.001f, FLT_MAX, st, ovf);
+  const HitInfo h = trace<false, MS>(S, ray, 0.001f, FLT_MAX, st, ovf);
   if (h.prim < 0) {
     if (G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * G.background_intensity;
     return true;
   }
-  const Surface sf = surface(S, ray, h);
+  const Surface sf = surface<MS>(S, ray, h);
   if (!sf.visible && bounce == 0) {  // camera rays pass through invisible geometry
     ray.o = sf.p + ray.d * 0.01f;
     return ++bounce >= max_depth;
   }
   if (sf.mat >= S.num_mats) return true;
   const DevMaterial &m = S.mats[sf.mat];
-  const ScatterOut so = scatter(G, m, sf, ray, key, bounce);
+  const ScatterOut so = scatter<MS>(G, m, sf, ray, key, bounce);
   if (so.emit.length_squared() > 0.0f) {
     float w = 1.0f;
     if (NEE && prev_pdf > 0.0f && m.kind == L_LIGHT && S.num_lights > 0) {
@@ -440,7 +452,7 @@ __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &
           Ray sr;
           sr.o = o;
           sr.d = wi;
-          const HitInfo sh = trace<true>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
+          const HitInfo sh = trace<true, MS>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
           if (sh.prim < 0) {
             const float pl = d2 / (cl * S.light_area);
             const float pb = cs * (1.0f / RB_PI);
@@ -468,8 +480,8 @@ __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &
 // runs its samples back to back in a single flattened loop (one path segment
 // per iteration), so a lane whose path ended starts its next sample at once
 // instead of idling until the warp's longest path finishes.
-template <bool NEE>
-__global__ void __launch_bounds__(256) k_render(SceneView S, Globals G, FrameF P, float4 *__restrict__ acc,
+template <bool NEE, int MS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_render(SceneView S, Globals G, FrameF P, float4 *__restrict__ acc,
                                                 float4 *__restrict__ comp, int *__restrict__ counts,
                                                 unsigned long long *__restrict__ counters) {
   extern __shared__ int2 smem[];
@@ -522,7 +534,7 @@ __global__ void __launch_bounds__(256) k_render(SceneView S, Globals G, FrameF P
         alive = true;
       }
       ++segs;
-      if (path_segment<NEE>(S, G, st, ovf, ray, thr, L, bounce, prev_pdf, key, P.max_depth)) {
+      if (path_segment<NEE, MS>(S, G, st, ovf, ray, thr, L, bounce, prev_pdf, key, P.max_depth)) {
         if (comp) {
           kahan_add(sx, cx, L.x);
           kahan_add(sy, cy, L.y);
@@ -663,17 +675,54 @@ int launch_primary(const DeviceScene *ds, const FrameF &P, int32_t *ids, float *
   return cuda_ok(cudaGetLastError(), "k_primary launch") ? RB_OK : RB_ERR_CUDA;
 }
 
+// Register budget (min resident blocks of 256 threads per SM) per material
+// class; rb_render_opts.reserved[0] overrides it (the autotuner's knob).
+// Defaults from a sweep on B200 (occupancy x block shape, per class).
+static int default_minb(int ms, bool nee) {
+  if (ms == RB_MS_DIFFUSE) return 3;
+  if (ms == RB_MS_CLASSIC) return 2;
+  return nee ? 1 : 2;
+}
+static void default_block(int ms, int &bx, int &by) {
+  bx = ms == RB_MS_FULL ? 32 : 16;
+  by = ms == RB_MS_FULL ? 4 : 8;
+}
+
+template <bool NEE, int MS>
+static void launch_ms(int minb, dim3 grd, dim3 blk, size_t sm, cudaStream_t st, const SceneView &S, const Globals &G,
+                      const FrameF &P, float4 *acc, float4 *comp, int *counts, unsigned long long *counters) {
+  switch (minb) {
+    case 1: k_render<NEE, MS, 1><<<grd, blk, sm, st>>>(S, G, P, acc, comp, counts, counters); break;
+    case 3: k_render<NEE, MS, 3><<<grd, blk, sm, st>>>(S, G, P, acc, comp, counts, counters); break;
+    case 4: k_render<NEE, MS, 4><<<grd, blk, sm, st>>>(S, G, P, acc, comp, counts, counters); break;
+    default: k_render<NEE, MS, 2><<<grd, blk, sm, st>>>(S, G, P, acc, comp, counts, counters); break;
+  }
+}
+
 int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, int *counts,
                   unsigned long long *counters, cudaStream_t st) {
   const rb_render_opts o = current_opts();
-  int bx = o.block_x > 0 ? o.block_x : 16, by = o.block_y > 0 ? o.block_y : 16;
-  if (bx * by > 256) { bx = 16; by = 16; }
+  const int ms = ds->ms;
+  int bx, by;
+  default_block(ms, bx, by);
+  if (o.block_x > 0 && o.block_y > 0 && o.block_x * o.block_y <= 256 && o.block_x * o.block_y >= 32) {
+    bx = o.block_x;
+    by = o.block_y;
+  }
   dim3 blk(bx, by), grd((P.width + bx - 1) / bx, (P.height + by - 1) / by);
   const size_t sm = sizeof(int2) * RB_SHORT * blk.x * blk.y;
-  if (G.nee)
-    k_render<true><<<grd, blk, sm, st>>>(ds->view, G, P, acc, comp, counts, counters);
-  else
-    k_render<false><<<grd, blk, sm, st>>>(ds->view, G, P, acc, comp, counts, counters);
+  const int minb = o.reserved[0] > 0 ? o.reserved[0] : default_minb(ms, G.nee != 0);
+#define RB_LAUNCH(NEE_, MS_) launch_ms<NEE_, MS_>(minb, grd, blk, sm, st, ds->view, G, P, acc, comp, counts, counters)
+  if (G.nee) {
+    if (ms == RB_MS_DIFFUSE) RB_LAUNCH(true, RB_MS_DIFFUSE);
+    else if (ms == RB_MS_CLASSIC) RB_LAUNCH(true, RB_MS_CLASSIC);
+    else RB_LAUNCH(true, RB_MS_FULL);
+  } else {
+    if (ms == RB_MS_DIFFUSE) RB_LAUNCH(false, RB_MS_DIFFUSE);
+    else if (ms == RB_MS_CLASSIC) RB_LAUNCH(false, RB_MS_CLASSIC);
+    else RB_LAUNCH(false, RB_MS_FULL);
+  }
+#undef RB_LAUNCH
   g_launches++;
   return cuda_ok(cudaGetLastError(), "k_render launch") ? RB_OK : RB_ERR_CUDA;
 }

@@ -145,6 +145,17 @@ struct ScatterOut {
   bool scattered;
 };
 
+// Material classes a kernel is specialised for (the host picks the smallest
+// class covering a scene's materials and primitive kinds):
+//   RB_MS_DIFFUSE  Lambert, light, constant, normals
+//   RB_MS_CLASSIC  + mirror, rough mirror, glass
+//   RB_MS_FULL     + GGX conductor, thin film, clear coat, patterns,
+//                  displaced spheres and SDF primitives
+#define RB_MS_DIFFUSE 1
+#define RB_MS_CLASSIC 2
+#define RB_MS_FULL 3
+
+template <int MS>
 __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMaterial &m, const Surface &s, const Ray &in,
                                               uint32_t key, int bounce) {
   ScatterOut o;
@@ -153,7 +164,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
   o.pdf = 0.0f;
   o.scattered = false;
   f3 color = m.color;
-  if (m.pattern == 1) color = fib_dots(m, color, s.p, s.center);
+  if (MS >= RB_MS_FULL && m.pattern == 1) color = fib_dots(m, color, s.p, s.center);
   const uint32_t d0 = rb_vdim(bounce, RB_SLOT_BSDF);
   switch (m.kind) {
     case L_LAMBERTIAN: {
@@ -168,6 +179,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       break;
     }
     case L_MIRROR: {
+      if (MS < RB_MS_CLASSIC) break;
       const f3 r = reflect(normalize(in.d), s.n);
       o.ray.o = s.p;
       o.ray.d = r;
@@ -176,6 +188,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       break;
     }
     case L_ROUGH_MIRROR: {
+      if (MS < RB_MS_CLASSIC) break;
       const f3 pn = normalize(s.n + (m.roughness * G.metal_fuzziness) * uniform_sphere(rb_draw(key, d0), rb_draw(key, d0 + 1)));
       const f3 r = reflect(normalize(in.d), pn);
       o.ray.o = s.p;
@@ -185,6 +198,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       break;
     }
     case L_GLASS: {
+      if (MS < RB_MS_CLASSIC) break;
       const f3 ud = normalize(in.d);
       const float ri = G.glass_ior;
       const float ratio = s.front ? (1.0f / ri) : ri;
@@ -211,6 +225,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       o.emit = 0.5f * (s.n + f3(1.0f, 1.0f, 1.0f));
       break;
     case L_ANISO_METAL: {
+      if (MS < RB_MS_FULL) break;
       const float aspect = sqrtf(fmaxf(1e-4f, 1.0f - 0.9f * m.anisotropy));
       const float r2 = m.roughness * m.roughness;
       const float ax = fmaxf(1e-4f, r2 / aspect), ay = fmaxf(1e-4f, r2 * aspect);
@@ -242,6 +257,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       break;
     }
     case L_THIN_FILM: {
+      if (MS < RB_MS_FULL) break;
       const f3 ud = normalize(in.d);
       const float ci = fmaxf(fabsf(dot(-ud, s.n)), 0.001f);
       const float n0 = m.ior, n1 = m.film_ior, dd = m.film_thickness;
@@ -281,6 +297,7 @@ __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMateria
       break;
     }
     case L_CLEAR_COAT: {
+      if (MS < RB_MS_FULL) break;
       const f3 ud = normalize(in.d);
       const float ct = fminf(dot(-ud, s.n), 1.0f);
       const float F = schlick(ct, m.ior);

@@ -110,20 +110,27 @@ def test_dropin_chunks_equal_single_launch(cuda):
 
 
 def test_invisible_geometry_passes_camera_rays(cuda):
+    # an invisible quad in front of a red sphere: camera rays pass through it at
+    # bounce 0 (cuda_raytracer.cuh:879-883), so the centre pixel is red
     from rayon_b200 import scene as S
     sc = S.SceneDescription()
     red = sc.add_material(S.constant((1, 0, 0)))
     blue = sc.add_material(S.constant((0, 0, 1)))
     sc.add_sphere((0, 0, -5), 1.0, red)
-    sc.add_sphere((0, 0, -2), 0.5, blue)
-    sc.set_visible(1, False)
+    q = sc.add_rectangle((-1, -1, -2), (2, 0, 0), (0, 2, 0), blue)
+    sc.set_visible(q, False)
     sc.build_bvh()
     ds = sc.upload()
     fr = S.camera_frame((0, 0, 0), (0, 0, -1), (0, 1, 0), 30.0, 9, 9)
     img = render.render_accumulate(ds, fr, 9, 9, 4, 4, background=0.0)
-    c = img[4, 4] / 4
-    np.testing.assert_allclose(c, [1, 0, 0], atol=1e-6)  # blue sphere skipped at bounce 0
+    np.testing.assert_allclose(img[4, 4] / 4, [1, 0, 0], atol=1e-6)
+    # visible again: the quad is what the camera sees
+    sc.set_visible(q, True)
+    ds2 = sc.upload()
+    img = render.render_accumulate(ds2, fr, 9, 9, 4, 4, background=0.0)
+    np.testing.assert_allclose(img[4, 4] / 4, [0, 0, 1], atol=1e-6)
     ds.free()
+    ds2.free()
 
 
 @pytest.mark.parametrize("name", ["cornell", "mixed_materials"])
