@@ -109,6 +109,20 @@ void convertAccumToDisplayCUDA(void *d_accum_buffer, unsigned char *display_imag
                                int height, int channels, int num_samples, float gamma,
                                void *d_pixel_sample_counts RB_DEFAULT(NULL));
 
+/* No counterpart in the reference. Same conversion and output as
+ * convertAccumToDisplayCUDA, for callers that cannot allocate device memory
+ * when they ask for a frame (device memory owned by another allocator or held
+ * to a fixed budget; loops that must avoid cudaMalloc's implicit device-wide
+ * synchronisation). The 8-bit image is staged in a fixed 8 MiB device array
+ * that is part of the library (held on every GPU that loads it until exit):
+ * width * height * channels above 8388608 is rejected with RB_ERR_CAPACITY.
+ * Allocates nothing. The array's device address is looked up on the first call
+ * per device (make that call before any stream capture). Calls share the array,
+ * so calls that overlap on the GPU race. Returns an rb_status. */
+int convertAccumToDisplayNoAlloc(void *d_accum_buffer, unsigned char *display_image, int width,
+                                 int height, int channels, int num_samples, float gamma,
+                                 void *d_pixel_sample_counts);
+
 /* Replace the adaptive-sampling buffer helpers (renderer_cuda_device.cuh:58-63;
  * renderer_cuda_device.cu:397-437). countConvergedPixels reduces on the device
  * and copies back one integer. */
