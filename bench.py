@@ -182,10 +182,17 @@ def main():
     ap.add_argument("--impl", default="rayon_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--small", action="store_true",
+                    help="profiling case for ncu: same frame at 16 spp, no e2e/baselines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.small:
+        WORKLOAD["spp"] = 16
+        args.no_cpu_baseline = True
+        args.no_reference_cuda = True
+        args.no_e2e = True
 
     import torch
     rank, world, local = dist_env()
@@ -255,7 +262,8 @@ def main():
     # ---- e2e: the drop-in call with host buffers, as the reference's offline renderer
     e2e = None
     h2d = d2h = 0
-    if True:
+    mean_rad = None
+    if not getattr(args, "no_e2e", False):
         torch.cuda.synchronize()
         e2e_times = []
         for i in range(max(1, min(3, args.steps))):

@@ -249,6 +249,88 @@ int rb_render_accumulate(const rb_cuda_scene *scene, int width, int height, cons
                          int samples_to_add, int sample_base, int max_depth, float *accum,
                          float *comp, uint64_t *counters, void *stream);
 
+/* Number of kernel launches this library has made (all entry points). */
+unsigned long long rb_launch_count(void);
+
+/* ======================================================================== */
+/* 4. Batched multi-job engine and serving loop (additions; the reference    */
+/*    renders one job per call, renderer_cuda_progressive_host.hpp:884-922)  */
+/* ======================================================================== */
+
+/* One render job. The scene is an index returned by rb_server_add_scene. */
+typedef struct rb_job_request {
+  int scene;
+  int width, height;
+  int spp;               /* total samples per pixel */
+  int max_depth;
+  double frame[21];      /* rb_camera_frame output */
+  float light_intensity, background_intensity, metal_fuzziness, glass_ior;
+  int dof_enabled;
+  float dof_aperture, dof_focus;
+  int nee;
+  uint32_t seed;         /* job key of the counter-based sample streams */
+  int fp64_accum;        /* 1: FP64 accumulation (always used above 65536 spp) */
+  double arrival_time;   /* seconds on the server clock (rb_server_run_trace) */
+} rb_job_request;
+
+/* Defaults for rb_job_request: the reference's __constant__ shading values. */
+void rb_job_default(rb_job_request *out);
+
+typedef struct rb_server_opts {
+  int64_t memory_budget_bytes;  /* HBM admission budget: accumulation + frame buffers */
+  int max_active_jobs;          /* slots of the batched launch (<= 1024) */
+  int64_t paths_per_iteration;  /* work quantum of one batched launch */
+  int max_spp_per_iteration;    /* per-job cap of samples per pixel per launch */
+  int use_graph;                /* 1: each iteration is a CUDA graph launch */
+  int frames_every;             /* > 0: write each active job's u8 frame every N iterations */
+  int occupancy;                /* resident 256-thread blocks per SM (0 = tuned) */
+  int reserved[3];
+} rb_server_opts;
+
+void rb_server_default_opts(rb_server_opts *out);
+
+typedef struct rb_job_status {
+  int state;             /* 0 queued, 1 active, 2 done, -1 rejected */
+  int spp_done;
+  double t_arrival, t_admit, t_done;  /* server clock, seconds */
+  int64_t device_bytes;
+} rb_job_status;
+
+typedef struct rb_server_stats {
+  int64_t jobs_done, jobs_rejected, iterations, frames;
+  int64_t paths, segments;
+  double device_seconds;   /* sum of iteration device times (CUDA events) */
+  double wall_seconds;     /* first arrival to last completion */
+  int64_t peak_device_bytes;
+  double p50_latency, p99_latency, mean_latency;  /* arrival -> done, seconds */
+} rb_server_stats;
+
+typedef struct rb_server rb_server;
+
+rb_server *rb_server_create(const rb_server_opts *opts, void *stream);
+void rb_server_destroy(rb_server *s);
+/* Keeps a device scene resident for the server's jobs; returns its index. */
+int rb_server_add_scene(rb_server *s, const rb_cuda_scene *scene);
+/* Queues a job (FIFO); returns its id (>= 0) or an rb_status. */
+int64_t rb_server_submit(rb_server *s, const rb_job_request *req);
+/* Admits queued jobs while slots and budget allow, runs one batched
+ * iteration over all active jobs, retires finished ones. Returns the number
+ * of jobs still active or queued (0 = idle), or an rb_status. */
+int rb_server_step(rb_server *s);
+int rb_server_job_status(rb_server *s, int64_t job, rb_job_status *out);
+/* Copies a job's radiance sums (w*h*3 FP32, true sum = sum - compensation
+ * or the FP64 sum rounded) and/or its latest u8 RGBA frame to host memory. */
+int rb_server_fetch(rb_server *s, int64_t job, float *rgb_sum, uint8_t *rgba_frame);
+/* Returns a finished job's device memory to the budget. */
+int rb_server_release(rb_server *s, int64_t job);
+/* Runs a whole request stream: requests are submitted when the server clock
+ * passes their arrival_time (realtime = 1) or all at once (0); finished jobs
+ * are released unless keep_results. latencies[n] (may be NULL) receives
+ * arrival -> done seconds. */
+int rb_server_run_trace(rb_server *s, const rb_job_request *reqs, int64_t n, int realtime, int keep_results,
+                        double *latencies);
+int rb_server_get_stats(rb_server *s, rb_server_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -145,3 +145,45 @@ def check(status: int, what: str = "") -> int:
     if status < 0:
         raise RuntimeError(f"{what} failed ({status}): {last_error()}")
     return status
+
+
+# --- batched engine / serving loop ---------------------------------------------
+class JobRequest(C.Structure):
+    _fields_ = [("scene", C.c_int), ("width", C.c_int), ("height", C.c_int), ("spp", C.c_int),
+                ("max_depth", C.c_int), ("frame", C.c_double * 21), ("light_intensity", C.c_float),
+                ("background_intensity", C.c_float), ("metal_fuzziness", C.c_float), ("glass_ior", C.c_float),
+                ("dof_enabled", C.c_int), ("dof_aperture", C.c_float), ("dof_focus", C.c_float), ("nee", C.c_int),
+                ("seed", C.c_uint32), ("fp64_accum", C.c_int), ("arrival_time", C.c_double)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_int64), ("max_active_jobs", C.c_int), ("paths_per_iteration", C.c_int64),
+                ("max_spp_per_iteration", C.c_int), ("use_graph", C.c_int), ("frames_every", C.c_int),
+                ("occupancy", C.c_int), ("reserved", C.c_int * 3)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int), ("spp_done", C.c_int), ("t_arrival", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("device_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_done", C.c_int64), ("jobs_rejected", C.c_int64), ("iterations", C.c_int64),
+                ("frames", C.c_int64), ("paths", C.c_int64), ("segments", C.c_int64),
+                ("device_seconds", C.c_double), ("wall_seconds", C.c_double), ("peak_device_bytes", C.c_int64),
+                ("p50_latency", C.c_double), ("p99_latency", C.c_double), ("mean_latency", C.c_double)]
+
+
+_sig("rb_job_default", None, C.POINTER(JobRequest))
+_sig("rb_server_default_opts", None, C.POINTER(ServerOpts))
+_sig("rb_server_create", vp, C.POINTER(ServerOpts), vp)
+_sig("rb_server_destroy", None, vp)
+_sig("rb_server_add_scene", C.c_int, vp, vp)
+_sig("rb_server_submit", C.c_int64, vp, C.POINTER(JobRequest))
+_sig("rb_server_step", C.c_int, vp)
+_sig("rb_server_job_status", C.c_int, vp, C.c_int64, C.POINTER(JobStatus))
+_sig("rb_server_fetch", C.c_int, vp, C.c_int64, c_float_p, c_uint8_p)
+_sig("rb_server_release", C.c_int, vp, C.c_int64)
+_sig("rb_server_run_trace", C.c_int, vp, C.POINTER(JobRequest), C.c_int64, C.c_int, C.c_int, c_double_p)
+_sig("rb_server_get_stats", C.c_int, vp, C.POINTER(ServerStats))
+_sig("convertAccumToDisplayNoAlloc", C.c_int, vp, c_uint8_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, vp)

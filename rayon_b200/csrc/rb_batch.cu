@@ -1,0 +1,733 @@
+// Batched multi-job engine and the serving loop.
+//
+// One persistent launch per iteration renders every active job: the
+// iteration's work is a list of pixel tasks (job, pixel, n samples) that warps
+// claim 32 at a time with one atomic per warp (ballot of the lanes that need
+// work). A lane runs its task's samples in the flattened segment loop of the
+// per-frame kernel and claims the next task the moment its pixel is done, so
+// lanes stay busy across task and job boundaries and one launch fills the GPU
+// whatever the jobs' sizes. A task owns its pixel for the launch, so the
+// pixel's sums are updated without atomics (Kahan in FP32, or FP64).
+//
+// The serving loop (rb_server_*) keeps scenes resident, admits queued jobs as
+// slots and the HBM budget allow (continuous batching: new jobs join the next
+// iteration while others are still running), gives every active job a share
+// of the iteration's path quantum, retires finished jobs and optionally writes
+// a u8 progressive frame per job. Each iteration (job-table upload, counter
+// reset, kernel) can be one CUDA graph launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "rb_path.cuh"
+
+namespace rb {
+
+extern std::atomic<unsigned long long> g_launches;
+DeviceScene *lookup_scene(const void *handle);
+
+struct __align__(16) BatchJob {
+  SceneView S;
+  FrameF P;          // P.samples = samples per pixel in this iteration
+  Globals G;
+  float4 *acc;       // FP32 sums (w*h) followed by Kahan compensation (w*h)
+  double *acc64;     // FP64 sums (w*h*4), or null
+  unsigned char *frame;  // u8 RGBA progressive frame or null
+  long long task_begin;  // first task of this job in the iteration
+  int spp_total;         // samples accumulated after this iteration (frame normalisation)
+  int pad[3];
+};
+
+struct BatchCtl {
+  unsigned long long next_task;
+  unsigned long long total_tasks;
+  unsigned long long segments;
+  unsigned long long paths;
+  unsigned long long overflow;
+  int njobs;
+  int job_offset;  // first job of this launch's class in the job table
+  int pad[4];
+};
+
+__device__ __forceinline__ int find_job(const BatchJob *__restrict__ jobs, int njobs, long long t) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&jobs[mid].task_begin) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int MS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict__ jobs, BatchCtl *__restrict__ ctl) {
+  extern __shared__ int2 smem[];
+  jobs += ctl->job_offset;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  Stack st;
+  st.sh = smem + tid;
+  st.stride = blockDim.x;
+  uint32_t ovf = 0;
+  const unsigned long long total = ctl->total_tasks;
+  const int njobs = ctl->njobs;
+  unsigned long long segs = 0, paths = 0;
+
+  bool have = false, done_all = false;
+  int j = 0, pix = 0, x = 0, y = 0, s = 0, nsamp = 0, bounce = 0;
+  bool alive = false;
+  Ray ray;
+  f3 thr(1.f, 1.f, 1.f), L(0.f, 0.f, 0.f);
+  float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, prev_pdf = 0.f;
+  uint32_t key = 0;
+  while (true) {
+    // claim tasks for idle lanes, one atomic per warp
+    const bool need = !have && !done_all;
+    const unsigned mask = __ballot_sync(0xffffffffu, need);
+    if (mask) {
+      unsigned long long base = 0;
+      const int leader = __ffs(mask) - 1;
+      if (lane == leader) base = atomicAdd(&ctl->next_task, (unsigned long long)__popc(mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const unsigned long long t = base + __popc(mask & ((1u << lane) - 1u));
+        if (t < total) {
+          j = find_job(jobs, njobs, (long long)t);
+          pix = (int)((long long)t - __ldg(&jobs[j].task_begin));
+          const int w = __ldg(&jobs[j].P.width);
+          x = pix % w;
+          y = pix / w;
+          nsamp = __ldg(&jobs[j].P.samples);
+          s = 0;
+          sx = sy = sz = cx = cy = cz = 0.f;
+          have = true;
+          alive = false;
+        } else {
+          done_all = true;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, have) == 0) break;  // every lane out of work
+    if (have) {
+      const BatchJob &J = jobs[j];
+      if (!alive) {
+        if (s < nsamp && J.P.max_depth > 0) {
+          key = rb_path_key(J.P.seed, J.P.salt, (uint32_t)pix, (uint32_t)(J.P.sample_base + s));
+          ++s;
+          ray = camera_ray(J.P, J.G, x, y, key);
+          thr = f3(1.f, 1.f, 1.f);
+          L = f3(0.f, 0.f, 0.f);
+          bounce = 0;
+          prev_pdf = 0.f;
+          alive = true;
+        } else {
+          // task complete: fold the samples into the pixel (this task owns it)
+          const int n = J.P.width * J.P.height;
+          if (J.acc64) {
+            double4 *a = reinterpret_cast<double4 *>(J.acc64) + pix;
+            double4 v = *a;
+            v.x += (double)sx - (double)cx;
+            v.y += (double)sy - (double)cy;
+            v.z += (double)sz - (double)cz;
+            *a = v;
+          } else {
+            float4 a = J.acc[pix], c = J.acc[n + pix];
+            kahan_add(a.x, c.x, sx - cx);
+            kahan_add(a.y, c.y, sy - cy);
+            kahan_add(a.z, c.z, sz - cz);
+            J.acc[pix] = a;
+            J.acc[n + pix] = c;
+          }
+          paths += (unsigned long long)nsamp;
+          have = false;
+        }
+      }
+      if (alive) {
+        ++segs;
+        if (path_segment<true, MS>(J.S, J.G, st, ovf, ray, thr, L, bounce, prev_pdf, key, J.P.max_depth)) {
+          kahan_add(sx, cx, L.x);
+          kahan_add(sy, cy, L.y);
+          kahan_add(sz, cz, L.z);
+          alive = false;
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    segs += __shfl_down_sync(0xffffffffu, segs, o);
+    paths += __shfl_down_sync(0xffffffffu, paths, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&ctl->segments, segs);
+    atomicAdd(&ctl->paths, paths);
+  }
+  if (ovf) atomicAdd(&ctl->overflow, (unsigned long long)ovf);
+}
+
+// u8 RGBA progressive frames of all jobs of the iteration (one thread per pixel of every job).
+__global__ void k_batch_frames(const BatchJob *__restrict__ jobs, const BatchCtl *__restrict__ ctl) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)ctl->total_tasks) return;
+  const int j = find_job(jobs, ctl->njobs, t);
+  const BatchJob &J = jobs[j];
+  if (!J.frame) return;
+  const int pix = (int)(t - J.task_begin);
+  const int n = J.P.width * J.P.height;
+  float r, g, b;
+  if (J.acc64) {
+    const double4 v = reinterpret_cast<const double4 *>(J.acc64)[pix];
+    r = (float)v.x; g = (float)v.y; b = (float)v.z;
+  } else {
+    const float4 a = J.acc[pix], c = J.acc[n + pix];
+    r = a.x - c.x; g = a.y - c.y; b = a.z - c.z;
+  }
+  const float inv = 1.0f / (float)max(J.spp_total, 1);
+  unsigned char *o = J.frame + 4 * (size_t)pix;
+  o[0] = (unsigned char)(256.0f * fminf(sqrtf(fmaxf(r * inv, 0.0f)), 0.999f));
+  o[1] = (unsigned char)(256.0f * fminf(sqrtf(fmaxf(g * inv, 0.0f)), 0.999f));
+  o[2] = (unsigned char)(256.0f * fminf(sqrtf(fmaxf(b * inv, 0.0f)), 0.999f));
+  o[3] = 255;
+}
+
+template <int MS>
+static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl) {
+  const size_t sm = sizeof(int2) * RB_SHORT * 256;
+  switch (minb) {
+    case 1: k_batch<MS, 1><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 3: k_batch<MS, 3><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 4: k_batch<MS, 4><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    default: k_batch<MS, 2><<<grid, 256, sm, st>>>(jobs, ctl); break;
+  }
+}
+
+static void launch_batch(int ms, int minb, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms) {
+  const int grid = sms * minb;  // persistent: exactly the resident blocks
+  if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE>(minb, grid, st, jobs, ctl);
+  else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC>(minb, grid, st, jobs, ctl);
+  else launch_batch_ms<RB_MS_FULL>(minb, grid, st, jobs, ctl);
+  g_launches++;
+}
+
+// ---------------------------------------------------------------------------
+// Serving loop
+// ---------------------------------------------------------------------------
+struct Job {
+  rb_job_request req;
+  int64_t id;
+  int state = 0;  // 0 queued, 1 active, 2 done, -1 rejected
+  int spp_done = 0;
+  double t_arrival = 0, t_admit = 0, t_done = 0;
+  float4 *acc = nullptr;
+  double *acc64 = nullptr;
+  unsigned char *frame = nullptr;
+  int64_t bytes = 0;
+};
+
+struct Server {
+  rb_server_opts o;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  int sms = 148;
+  std::vector<const DeviceScene *> scenes;
+  std::unordered_map<int64_t, Job> jobs;
+  std::deque<int64_t> queue;
+  std::vector<int64_t> active;
+  int64_t next_id = 0;
+  int64_t used_bytes = 0, peak_bytes = 0;
+  BatchJob *h_jobs = nullptr;  // pinned
+  BatchJob *d_jobs = nullptr;
+  BatchCtl *h_ctl = nullptr;   // pinned
+  BatchCtl *d_ctl = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_frames = -1;
+  double aging = 0.5;  // priority = remaining paths / (1 + aging * seconds waited)
+  std::chrono::steady_clock::time_point t0;
+  rb_server_stats stats;
+  std::vector<double> latencies;
+  double first_arrival = -1, last_done = 0;
+
+  double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+static int64_t job_bytes(const rb_job_request &r, bool frames) {
+  const int64_t n = (int64_t)r.width * r.height;
+  const bool f64 = r.fp64_accum || r.spp > 65536;
+  return (f64 ? n * 32 : n * 32) + (frames ? n * 4 : 0);
+}
+
+static bool admit(Server &S, Job &J) {
+  const bool frames = S.o.frames_every > 0;
+  const int64_t need = job_bytes(J.req, frames);
+  if (S.used_bytes + need > S.o.memory_budget_bytes || (int)S.active.size() >= S.o.max_active_jobs) return false;
+  const int64_t n = (int64_t)J.req.width * J.req.height;
+  const bool f64 = J.req.fp64_accum || J.req.spp > 65536;
+  cudaError_t e;
+  if (f64) {
+    e = cudaMallocAsync((void **)&J.acc64, n * 32, S.st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(J.acc64, 0, n * 32, S.st);
+  } else {
+    e = cudaMallocAsync((void **)&J.acc, n * 32, S.st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(J.acc, 0, n * 32, S.st);
+  }
+  if (e == cudaSuccess && frames) {
+    e = cudaMallocAsync((void **)&J.frame, n * 4, S.st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(J.frame, 0, n * 4, S.st);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (J.acc) cudaFreeAsync(J.acc, S.st);
+    if (J.acc64) cudaFreeAsync(J.acc64, S.st);
+    if (J.frame) cudaFreeAsync(J.frame, S.st);
+    J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr;
+    return false;
+  }
+  J.bytes = need;
+  S.used_bytes += need;
+  S.peak_bytes = std::max(S.peak_bytes, S.used_bytes);
+  J.state = 1;
+  J.t_admit = S.now();
+  S.active.push_back(J.id);
+  return true;
+}
+
+static void free_job(Server &S, Job &J) {
+  if (J.acc) cudaFreeAsync(J.acc, S.st);
+  if (J.acc64) cudaFreeAsync(J.acc64, S.st);
+  if (J.frame) cudaFreeAsync(J.frame, S.st);
+  J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr;
+  S.used_bytes -= J.bytes;
+  J.bytes = 0;
+}
+
+static int server_step(Server &S) {
+  // admission: FIFO while slots and memory allow
+  while (!S.queue.empty()) {
+    Job &J = S.jobs[S.queue.front()];
+    if (!admit(S, J)) {
+      if (S.active.empty()) {  // can never fit: reject instead of blocking the queue
+        J.state = -1;
+        S.stats.jobs_rejected++;
+        S.queue.pop_front();
+        continue;
+      }
+      break;
+    }
+    S.queue.pop_front();
+  }
+  if (S.active.empty()) return (int)S.queue.size();
+  // Plan: shortest remaining work first, aged by waiting time so large jobs
+  // are not starved, until the iteration's path quantum is used; each planned
+  // job gets as many samples per pixel as fit (capped), so tasks are long and
+  // an iteration holds few scenes.
+  const double tnow = S.now();
+  struct Plan { int64_t id; int spp; int cls; double prio; };
+  std::vector<Plan> cand;
+  for (int64_t id : S.active) {
+    Job &J = S.jobs[id];
+    const double rem = (double)J.req.width * J.req.height * (J.req.spp - J.spp_done);
+    const double age = tnow - J.t_arrival;
+    cand.push_back({id, 0, S.scenes[J.req.scene]->ms, rem / (1.0 + S.aging * age)});
+  }
+  std::stable_sort(cand.begin(), cand.end(), [](const Plan &a, const Plan &b) { return a.prio < b.prio; });
+  int64_t budget = S.o.paths_per_iteration;
+  std::vector<Plan> plan;
+  for (Plan &c : cand) {
+    if (budget <= 0 && !plan.empty()) break;
+    Job &J = S.jobs[c.id];
+    const int64_t px = (int64_t)J.req.width * J.req.height;
+    int64_t q = std::max<int64_t>(1, budget / std::max<int64_t>(px, 1));
+    q = std::min<int64_t>(q, S.o.max_spp_per_iteration);
+    q = std::min<int64_t>(q, J.req.spp - J.spp_done);
+    c.spp = (int)q;
+    budget -= q * px;
+    plan.push_back(c);
+  }
+  // group by kernel class (each class runs its own specialised persistent
+  // kernel, so a job's code and results do not depend on the mix); within a
+  // class, more samples per task first
+  std::stable_sort(plan.begin(), plan.end(), [](const Plan &a, const Plan &b) {
+    return a.cls != b.cls ? a.cls < b.cls : a.spp > b.spp;
+  });
+  long long tb = 0;
+  std::memset(S.h_ctl, 0, sizeof(BatchCtl) * 4);
+  int jfirst[4] = {0, 0, 0, 0};
+  for (size_t k = 0; k < plan.size(); ++k) {
+    Job &J = S.jobs[plan[k].id];
+    const DeviceScene *ds = S.scenes[J.req.scene];
+    const int cls = plan[k].cls;
+    BatchCtl &C = S.h_ctl[cls];
+    if (C.njobs == 0) {
+      jfirst[cls] = (int)k;
+      C.next_task = (unsigned long long)tb;
+    }
+    C.njobs++;
+    BatchJob &B = S.h_jobs[k];
+    std::memset(&B, 0, sizeof B);
+    B.S = ds->view;
+    B.P = frame_from(J.req.frame, J.req.width, J.req.height);
+    B.P.samples = plan[k].spp;
+    B.P.sample_base = J.spp_done;
+    B.P.max_depth = J.req.max_depth;
+    B.P.seed = current_opts().seed;
+    B.P.salt = J.req.seed;
+    B.G.light_intensity = J.req.light_intensity;
+    B.G.background_intensity = J.req.background_intensity;
+    B.G.metal_fuzziness = J.req.metal_fuzziness;
+    B.G.glass_ior = J.req.glass_ior;
+    B.G.dof_enabled = J.req.dof_enabled;
+    B.G.dof_aperture = J.req.dof_aperture;
+    B.G.dof_focus = J.req.dof_focus;
+    B.G.nee = J.req.nee;
+    B.acc = J.acc;
+    B.acc64 = J.acc64;
+    B.task_begin = tb;
+    B.spp_total = J.spp_done + plan[k].spp;
+    const bool frame_now = S.o.frames_every > 0 && ((S.stats.iterations + 1) % S.o.frames_every == 0 ||
+                                                     B.spp_total >= J.req.spp);
+    B.frame = frame_now ? J.frame : nullptr;
+    tb += (long long)J.req.width * J.req.height;
+    C.total_tasks = (unsigned long long)tb;
+  }
+  for (int c = 1; c <= 3; ++c) S.h_ctl[c].job_offset = jfirst[c];
+  S.h_ctl[0].total_tasks = (unsigned long long)tb;             // all jobs (frames)
+  S.h_ctl[0].njobs = (int)plan.size();
+  const bool frames = S.o.frames_every > 0;
+  auto minb_of = [&](int cls) {
+    if (S.o.occupancy > 0) return S.o.occupancy;
+    return cls == RB_MS_DIFFUSE ? 3 : 2;
+  };
+  auto kernels = [&](bool all_classes) {
+    for (int c = 1; c <= 3; ++c)
+      if (all_classes || S.h_ctl[c].njobs > 0)
+        launch_batch(c, minb_of(c), S.st, S.d_jobs, S.d_ctl + c, S.sms);
+  };
+  const long long frame_blocks_cap = (S.o.paths_per_iteration + 255) / 256 + 1;
+  cudaEventRecord(S.ev0, S.st);
+  if (S.o.use_graph && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
+    // One graph, reused every iteration: table and control blocks are copied
+    // from pinned staging when the graph runs, the three class kernels are
+    // persistent (grid = resident blocks) and exit at once when their class
+    // has no work this iteration.
+    if (!S.graph || S.graph_frames != (int)frames) {
+      if (S.graph) cudaGraphExecDestroy(S.graph);
+      S.graph = nullptr;
+      cudaGraph_t g;
+      if (!cuda_ok(cudaStreamBeginCapture(S.st, cudaStreamCaptureModeThreadLocal), "graph capture")) return RB_ERR_CUDA;
+      cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * S.o.max_active_jobs, cudaMemcpyHostToDevice, S.st);
+      cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * 4, cudaMemcpyHostToDevice, S.st);
+      for (int c = 1; c <= 3; ++c) launch_batch(c, minb_of(c), S.st, S.d_jobs, S.d_ctl + c, S.sms);
+      if (frames) k_batch_frames<<<(unsigned)frame_blocks_cap, 256, 0, S.st>>>(S.d_jobs, S.d_ctl);
+      if (!cuda_ok(cudaStreamEndCapture(S.st, &g), "graph capture")) return RB_ERR_CUDA;
+      if (!cuda_ok(cudaGraphInstantiate(&S.graph, g, 0), "graph instantiate")) return RB_ERR_CUDA;
+      cudaGraphDestroy(g);
+      S.graph_frames = (int)frames;
+    }
+    if (!cuda_ok(cudaGraphLaunch(S.graph, S.st), "graph launch")) return RB_ERR_CUDA;
+    g_launches += 3 + (frames ? 1 : 0);
+  } else {
+    cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
+    cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * 4, cudaMemcpyHostToDevice, S.st);
+    kernels(false);
+    if (frames) {
+      k_batch_frames<<<(unsigned)((tb + 255) / 256), 256, 0, S.st>>>(S.d_jobs, S.d_ctl);
+      g_launches++;
+    }
+  }
+  cudaEventRecord(S.ev1, S.st);
+  cudaMemcpyAsync(S.h_ctl, S.d_ctl, sizeof(BatchCtl) * 4, cudaMemcpyDeviceToHost, S.st);
+  if (!cuda_ok(cudaStreamSynchronize(S.st), "batched iteration")) return RB_ERR_CUDA;
+  float ms_it = 0.f;
+  cudaEventElapsedTime(&ms_it, S.ev0, S.ev1);
+  S.stats.device_seconds += ms_it * 1e-3;
+  S.stats.iterations++;
+  for (int c = 1; c <= 3; ++c) {
+    S.stats.paths += (int64_t)S.h_ctl[c].paths;
+    S.stats.segments += (int64_t)S.h_ctl[c].segments;
+  }
+  if (frames) S.stats.frames += (int64_t)plan.size();
+  // retire
+  const double t = S.now();
+  std::vector<int64_t> still;
+  std::unordered_map<int64_t, int> got;
+  for (const Plan &p : plan) got[p.id] = p.spp;
+  for (int64_t id : S.active) {
+    Job &J = S.jobs[id];
+    auto it = got.find(id);
+    if (it != got.end()) J.spp_done += it->second;
+    if (J.spp_done >= J.req.spp) {
+      J.state = 2;
+      J.t_done = t;
+      S.stats.jobs_done++;
+      S.latencies.push_back(J.t_done - J.t_arrival);
+      S.last_done = t;
+    } else {
+      still.push_back(id);
+    }
+  }
+  S.active.swap(still);
+  return (int)(S.active.size() + S.queue.size());
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+struct rb_server {
+  Server s;
+};
+
+extern "C" {
+
+void rb_job_default(rb_job_request *r) {
+  if (!r) return;
+  std::memset(r, 0, sizeof *r);
+  r->max_depth = 16;
+  r->spp = 1;
+  r->light_intensity = 1.0f;
+  r->background_intensity = 1.0f;
+  r->metal_fuzziness = 0.8f;
+  r->glass_ior = 1.5f;
+  r->dof_aperture = 0.1f;
+  r->dof_focus = 10.0f;
+}
+
+void rb_server_default_opts(rb_server_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->memory_budget_bytes = (int64_t)150 << 30;
+  o->max_active_jobs = 256;
+  o->paths_per_iteration = 64ll << 20;
+  o->max_spp_per_iteration = 64;
+  o->use_graph = 1;
+  o->frames_every = 0;
+}
+
+rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
+  rb_server *r = new rb_server();
+  Server &S = r->s;
+  rb_server_default_opts(&S.o);
+  if (opts) S.o = *opts;
+  if (S.o.max_active_jobs <= 0 || S.o.max_active_jobs > 1024 || S.o.paths_per_iteration <= 0 ||
+      S.o.max_spp_per_iteration <= 0 || S.o.memory_budget_bytes <= 0) {
+    set_error("rb_server_create: invalid options");
+    delete r;
+    return nullptr;
+  }
+  S.st = static_cast<cudaStream_t>(stream);
+  if (!S.st) {
+    cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking);
+    S.own_stream = true;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&S.sms, cudaDevAttrMultiProcessorCount, dev);
+  bool ok = cuda_ok(cudaMallocHost(&S.h_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server pinned jobs") &&
+            cuda_ok(cudaMalloc(&S.d_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server jobs") &&
+            cuda_ok(cudaMallocHost(&S.h_ctl, sizeof(BatchCtl) * 4), "server pinned ctl") &&
+            cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * 4), "server ctl");
+  if (!ok) {
+    rb_server_destroy(r);
+    return nullptr;
+  }
+  std::memset(S.h_jobs, 0, sizeof(BatchJob) * S.o.max_active_jobs);
+  cudaEventCreate(&S.ev0);
+  cudaEventCreate(&S.ev1);
+  std::memset(&S.stats, 0, sizeof S.stats);
+  S.t0 = std::chrono::steady_clock::now();
+  return r;
+}
+
+void rb_server_destroy(rb_server *r) {
+  if (!r) return;
+  Server &S = r->s;
+  if (S.st) cudaStreamSynchronize(S.st);
+  for (auto &kv : S.jobs) free_job(S, kv.second);
+  if (S.st) cudaStreamSynchronize(S.st);
+  if (S.graph) cudaGraphExecDestroy(S.graph);
+  if (S.h_jobs) cudaFreeHost(S.h_jobs);
+  if (S.d_jobs) cudaFree(S.d_jobs);
+  if (S.h_ctl) cudaFreeHost(S.h_ctl);
+  if (S.d_ctl) cudaFree(S.d_ctl);
+  if (S.ev0) cudaEventDestroy(S.ev0);
+  if (S.ev1) cudaEventDestroy(S.ev1);
+  if (S.own_stream && S.st) cudaStreamDestroy(S.st);
+  delete r;
+}
+
+int rb_server_add_scene(rb_server *r, const rb_cuda_scene *scene) {
+  if (!r) return RB_ERR_INVALID_ARG;
+  const DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_server_add_scene: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  r->s.scenes.push_back(ds);
+  return (int)r->s.scenes.size() - 1;
+}
+
+int64_t rb_server_submit(rb_server *r, const rb_job_request *q) {
+  if (!r || !q) return RB_ERR_INVALID_ARG;
+  Server &S = r->s;
+  if (q->scene < 0 || q->scene >= (int)S.scenes.size() || q->width <= 0 || q->height <= 0 || q->spp <= 0 ||
+      q->max_depth < 0 || (int64_t)q->width * q->height > (1ll << 31) - 1) {
+    set_error("rb_server_submit: invalid request");
+    return RB_ERR_INVALID_ARG;
+  }
+  Job J;
+  J.req = *q;
+  J.id = S.next_id++;
+  J.t_arrival = S.now();
+  if (S.first_arrival < 0) S.first_arrival = J.t_arrival;
+  S.jobs.emplace(J.id, J);
+  S.queue.push_back(J.id);
+  return J.id;
+}
+
+int rb_server_step(rb_server *r) {
+  if (!r) return RB_ERR_INVALID_ARG;
+  return server_step(r->s);
+}
+
+int rb_server_job_status(rb_server *r, int64_t id, rb_job_status *out) {
+  if (!r || !out) return RB_ERR_INVALID_ARG;
+  auto it = r->s.jobs.find(id);
+  if (it == r->s.jobs.end()) return RB_ERR_NOT_FOUND;
+  const Job &J = it->second;
+  out->state = J.state;
+  out->spp_done = J.spp_done;
+  out->t_arrival = J.t_arrival;
+  out->t_admit = J.t_admit;
+  out->t_done = J.t_done;
+  out->device_bytes = J.bytes;
+  return RB_OK;
+}
+
+int rb_server_fetch(rb_server *r, int64_t id, float *rgb, uint8_t *frame) {
+  if (!r) return RB_ERR_INVALID_ARG;
+  Server &S = r->s;
+  auto it = S.jobs.find(id);
+  if (it == S.jobs.end()) return RB_ERR_NOT_FOUND;
+  Job &J = it->second;
+  if (!J.acc && !J.acc64) {
+    set_error("rb_server_fetch: job has no device buffers (queued, rejected or released)");
+    return RB_ERR_STATE;
+  }
+  cudaStreamSynchronize(S.st);
+  const int64_t n = (int64_t)J.req.width * J.req.height;
+  if (rgb) {
+    if (J.acc64) {
+      std::vector<double> h(n * 4);
+      if (!cuda_ok(cudaMemcpy(h.data(), J.acc64, n * 32, cudaMemcpyDeviceToHost), "fetch")) return RB_ERR_CUDA;
+      for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) rgb[3 * i + k] = (float)h[4 * i + k];
+    } else {
+      std::vector<float> h(n * 8);
+      if (!cuda_ok(cudaMemcpy(h.data(), J.acc, n * 32, cudaMemcpyDeviceToHost), "fetch")) return RB_ERR_CUDA;
+      for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) rgb[3 * i + k] = (float)((double)h[4 * i + k] - (double)h[4 * (n + i) + k]);
+    }
+  }
+  if (frame) {
+    if (!J.frame) {
+      set_error("rb_server_fetch: frames are off (rb_server_opts.frames_every = 0)");
+      return RB_ERR_STATE;
+    }
+    if (!cuda_ok(cudaMemcpy(frame, J.frame, n * 4, cudaMemcpyDeviceToHost), "fetch frame")) return RB_ERR_CUDA;
+  }
+  return RB_OK;
+}
+
+int rb_server_release(rb_server *r, int64_t id) {
+  if (!r) return RB_ERR_INVALID_ARG;
+  auto it = r->s.jobs.find(id);
+  if (it == r->s.jobs.end()) return RB_ERR_NOT_FOUND;
+  if (it->second.state == 1) {
+    set_error("rb_server_release: job is still active");
+    return RB_ERR_STATE;
+  }
+  free_job(r->s, it->second);
+  return RB_OK;
+}
+
+int rb_server_run_trace(rb_server *r, const rb_job_request *reqs, int64_t n, int realtime, int keep, double *lat) {
+  if (!r || (!reqs && n > 0) || n < 0) return RB_ERR_INVALID_ARG;
+  Server &S = r->s;
+  std::vector<int64_t> ids(n, -1);
+  std::vector<int64_t> order(n);
+  for (int64_t i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int64_t a, int64_t b) { return reqs[a].arrival_time < reqs[b].arrival_time; });
+  const double base = S.now();
+  int64_t next = 0;
+  std::vector<char> released(n, 0);
+  while (true) {
+    const double t = S.now() - base;
+    while (next < n && (!realtime || reqs[order[next]].arrival_time <= t)) {
+      const int64_t k = order[next];
+      const int64_t id = rb_server_submit(r, &reqs[k]);
+      if (id < 0) return (int)id;
+      if (realtime) S.jobs[id].t_arrival = base + reqs[k].arrival_time;  // nominal arrival
+      ids[k] = id;
+      ++next;
+    }
+    const int left = server_step(S);
+    if (left < 0) return left;
+    if (!keep)
+      for (int64_t k = 0; k < n; ++k)
+        if (ids[k] >= 0 && !released[k] && S.jobs[ids[k]].state == 2) {
+          free_job(S, S.jobs[ids[k]]);
+          released[k] = 1;
+        }
+    if (left == 0 && next >= n) break;
+    if (left == 0 && realtime && next < n) {
+      // idle until the next arrival
+      const double wait = reqs[order[next]].arrival_time - (S.now() - base);
+      if (wait > 0) {
+        auto until = std::chrono::steady_clock::now() + std::chrono::duration<double>(wait);
+        while (std::chrono::steady_clock::now() < until) {
+        }
+      }
+    }
+  }
+  if (lat)
+    for (int64_t k = 0; k < n; ++k) {
+      const Job &J = S.jobs[ids[k]];
+      lat[k] = J.state == 2 ? J.t_done - J.t_arrival : -1.0;
+    }
+  return RB_OK;
+}
+
+int rb_server_get_stats(rb_server *r, rb_server_stats *out) {
+  if (!r || !out) return RB_ERR_INVALID_ARG;
+  Server &S = r->s;
+  *out = S.stats;
+  out->peak_device_bytes = S.peak_bytes;
+  out->wall_seconds = S.first_arrival >= 0 ? S.last_done - S.first_arrival : 0.0;
+  std::vector<double> l = S.latencies;
+  if (!l.empty()) {
+    std::sort(l.begin(), l.end());
+    auto q = [&](double p) {
+      const double idx = p * (l.size() - 1);
+      const size_t i = (size_t)idx;
+      const double f = idx - i;
+      return i + 1 < l.size() ? l[i] * (1 - f) + l[i + 1] * f : l[i];
+    };
+    out->p50_latency = q(0.5);
+    out->p99_latency = q(0.99);
+    double sum = 0;
+    for (double v : l) sum += v;
+    out->mean_latency = sum / l.size();
+  }
+  return RB_OK;
+}
+
+}  // extern "C"

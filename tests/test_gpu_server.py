@@ -1,0 +1,148 @@
+"""Batched multi-job engine and serving loop: each job's result is the same
+alone and in a mix, agrees with the per-frame kernel on the same sample
+streams, admission respects the HBM budget, FP64 accumulation, progressive
+frames and trace latencies."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+from cases import mixed_materials  # noqa: E402
+
+from rayon_b200 import render, scenes, serving  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+# alone vs mixed: only the grouping of samples into Kahan-compensated FP32
+# partial sums differs (each iteration's share of samples depends on the mix)
+RTOL, ATOL_PER_SPP = 2e-5, 2e-5
+
+
+def _scenes():
+    out = []
+    for spec in (scenes.cornell(), scenes.one_weekend(), mixed_materials()):
+        sc = spec.to_scene()
+        sc.build_bvh()
+        out.append((spec, sc, sc.upload()))
+    return out
+
+
+def _jobs(server_ids, specs):
+    reqs = []
+    dims = [(64, 64, 64), (80, 45, 48), (48, 36, 32), (96, 96, 16), (40, 30, 100)]
+    for k, (w, h, spp) in enumerate(dims):
+        si = k % len(specs)
+        spec = specs[si][0]
+        reqs.append((serving.job(server_ids[si], spec.camera.frame(w, h), w, h, spp, spec.depth,
+                                 background=spec.background, dof=spec.dof, nee=(k == 4), seed=1000 + k), w, h, spp))
+    return reqs
+
+
+def test_same_alone_and_in_mix(cuda):
+    S = _scenes()
+    mix = serving.Server(paths_per_iteration=200_000, max_spp_per_iteration=16)
+    ids = [mix.add_scene(ds) for _, _, ds in S]
+    reqs = _jobs(ids, S)
+    jids = [mix.submit(r) for r, *_ in reqs]
+    mix.drain()
+    for (r, w, h, spp), jid in zip(reqs, jids):
+        st = mix.status(jid)
+        assert st.state == 2 and st.spp_done == spp
+        got = mix.fetch(jid, w, h)
+        alone = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=64)
+        aid = [alone.add_scene(ds) for _, _, ds in S]
+        r.scene = aid[r.scene]
+        a = alone.submit(r)
+        alone.drain()
+        ref = alone.fetch(a, w, h)
+        np.testing.assert_allclose(got, ref, rtol=RTOL, atol=ATOL_PER_SPP * spp)
+        alone.close()
+    mix.close()
+
+
+def test_server_matches_per_frame_kernel(cuda):
+    spec = scenes.cornell(width=64, height=64)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    srv = serving.Server(paths_per_iteration=64 * 64 * 8)
+    sid = srv.add_scene(ds)
+    fr = spec.camera.frame(64, 64)
+    j = srv.submit(serving.job(sid, fr, 64, 64, 32, spec.depth, background=0.0, seed=0))
+    srv.drain()
+    got = srv.fetch(j, 64, 64)
+    ref = render.render_accumulate(ds, fr, 64, 64, 32, spec.depth, background=0.0)  # same streams (salt 0)
+    np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-4 * 32)
+    srv.close()
+
+
+def test_admission_budget_and_rejection(cuda):
+    S = _scenes()
+    # room for two 64x64 jobs (32 B per pixel each) but not three
+    srv = serving.Server(budget_bytes=2 * 64 * 64 * 32 + 100, paths_per_iteration=64 * 64 * 4)
+    sid = srv.add_scene(S[0][2])
+    spec = S[0][0]
+    fr = spec.camera.frame(64, 64)
+    jids = [srv.submit(serving.job(sid, fr, 64, 64, 16, 8, background=0.0, seed=k)) for k in range(5)]
+    big = srv.submit(serving.job(sid, spec.camera.frame(512, 512), 512, 512, 4, 8, background=0.0))
+    peak_active = 0
+    while True:
+        left = srv.step()
+        active = sum(srv.status(j).state == 1 for j in jids)
+        peak_active = max(peak_active, active)
+        for j in jids:
+            if srv.status(j).state == 2:
+                srv.release(j) if srv.status(j).device_bytes else None
+        if left == 0:
+            break
+    assert peak_active <= 2
+    assert all(srv.status(j).state == 2 for j in jids)
+    assert srv.status(big).state == -1  # can never fit the budget
+    st = srv.stats()
+    assert st.peak_device_bytes <= 2 * 64 * 64 * 32 + 100
+    assert st.jobs_rejected == 1
+    srv.close()
+
+
+def test_fp64_accumulation_and_frames(cuda):
+    spec = scenes.cornell(width=48, height=48)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    srv = serving.Server(paths_per_iteration=48 * 48 * 8, frames_every=1)
+    sid = srv.add_scene(ds)
+    fr = spec.camera.frame(48, 48)
+    a = srv.submit(serving.job(sid, fr, 48, 48, 40, spec.depth, background=0.0, seed=7))
+    b = srv.submit(serving.job(sid, fr, 48, 48, 40, spec.depth, background=0.0, seed=7, fp64=True))
+    srv.drain()
+    ra, fa = srv.fetch(a, 48, 48, frame=True)
+    rb, fb = srv.fetch(b, 48, 48, frame=True)
+    np.testing.assert_allclose(ra, rb, rtol=1e-5, atol=1e-4)
+    expect = (256 * np.minimum(np.sqrt(np.maximum(ra / 40, 0)), 0.999)).astype(np.uint8)
+    assert np.abs(fa[..., :3].astype(int) - expect).max() <= 1
+    assert (fa[..., 3] == 255).all()
+    assert srv.stats().frames >= 2
+    srv.close()
+
+
+def test_trace_latencies(cuda):
+    S = _scenes()
+    srv = serving.Server(paths_per_iteration=1 << 20)
+    ids = [srv.add_scene(ds) for _, _, ds in S]
+    reqs = []
+    rng = np.random.default_rng(0)
+    t = 0.0
+    for k in range(30):
+        t += rng.exponential(1 / 200.0)
+        si = k % 3
+        spec = S[si][0]
+        reqs.append(serving.job(ids[si], spec.camera.frame(64, 48), 64, 48, int(rng.integers(4, 32)), spec.depth,
+                                background=spec.background, dof=spec.dof, seed=k, arrival=t))
+    lat = srv.run_trace(reqs, realtime=True)
+    assert (lat > 0).all()
+    st = srv.stats()
+    assert st.jobs_done == 30 and st.p99_latency >= st.p50_latency > 0
+    assert st.paths == sum(r.width * r.height * r.spp for r in reqs)
+    srv.close()
