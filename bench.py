@@ -208,7 +208,8 @@ def main():
     paths = w * h * spp
     sc = spec.to_scene()
     sc.build_bvh()
-    ds = sc.upload()
+    ds = sc.upload(layout="autotune", tune_depth=depth)
+    layout = ds.layout
     fr = np.ascontiguousarray(spec.camera.frame(w, h), np.float64)
     frp = fr.ctypes.data_as(C.POINTER(C.c_double))
     render.set_globals(background=spec.background)
@@ -268,7 +269,7 @@ def main():
         e2e_times = []
         for i in range(max(1, min(3, args.steps))):
             t0 = time.perf_counter()
-            ds2 = sc.upload()
+            ds2 = sc.upload(layout="autotune", tune_depth=depth)  # tuning decision cached per scene
             img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
             ds2.free()
             torch.cuda.synchronize()
@@ -295,6 +296,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"cornell {w}x{h}, {spp} spp, depth {depth}, 30 primitives, background 0",
                    "paths_per_step": paths, "kernel": "k_render (per-pixel, flattened sample x bounce loop)",
+                   "layout": layout,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "mrays_per_s": world * segs / (t_ms * 1e-3) / 1e6,
         "segments_per_path": segs / max(npaths, 1),

@@ -212,8 +212,22 @@ void rb_camera_frame(const double look_from[3], const double look_at[3], const d
 typedef struct rb_upload_opts {
   int quantized_bvh;   /* 1: 8-bit child bounds relative to the parent */
   int use_bvh;         /* 0: linear scan (reference use_bvh == false)   */
-  int reserved[6];
+  int layout;          /* RB_LAYOUT_*: how the render kernels see the scene */
+  int max_leaf;        /* RB_LAYOUT_LEAF: BVH leaf size to rebuild with */
+  int tune_depth;      /* path depth of the autotuner's probe (0 = 8) */
+  int reserved[3];
 } rb_upload_opts;
+
+/* RB_LAYOUT_AS_BUILT: the scene's BVH as built (the reference's leaf-4 tree
+ * from rb_scene_build_bvh: primary-hit ids bit-exact against the reference).
+ * RB_LAYOUT_AUTOTUNE: time a probe render on each candidate layout (linear
+ * scan for small scenes, BVH leaf sizes 1/2/4/8) and keep the fastest.
+ * RB_LAYOUT_LINEAR: no BVH. RB_LAYOUT_LEAF: rebuild the BVH with max_leaf. */
+enum { RB_LAYOUT_AS_BUILT = 0, RB_LAYOUT_AUTOTUNE = 1, RB_LAYOUT_LINEAR = 2, RB_LAYOUT_LEAF = 3 };
+
+/* Layout the upload chose: kind (RB_LAYOUT_LINEAR or RB_LAYOUT_LEAF),
+ * leaf size (0 for linear) and, when autotuned, the probe time of the winner. */
+int rb_scene_layout_info(const rb_cuda_scene *scene, int *kind, int *leaf, float *probe_ms);
 
 /* Upload to the current device. Returns an opaque device-scene handle that is
  * also accepted wherever the drop-in group takes a CudaScene::Scene*. */

@@ -54,7 +54,11 @@ class MaterialDesc(C.Structure):
 
 
 class UploadOpts(C.Structure):
-    _fields_ = [("quantized_bvh", C.c_int), ("use_bvh", C.c_int), ("reserved", C.c_int * 6)]
+    _fields_ = [("quantized_bvh", C.c_int), ("use_bvh", C.c_int), ("layout", C.c_int), ("max_leaf", C.c_int),
+                ("tune_depth", C.c_int), ("reserved", C.c_int * 3)]
+
+
+LAYOUT_AS_BUILT, LAYOUT_AUTOTUNE, LAYOUT_LINEAR, LAYOUT_LEAF = 0, 1, 2, 3
 
 
 class RenderOpts(C.Structure):
@@ -130,6 +134,7 @@ _sig("rb_camera_frame", None, c_double_p, c_double_p, c_double_p, C.c_double, C.
 _sig("rb_scene_upload", vp, vp, C.POINTER(UploadOpts), vp)
 _sig("rb_scene_free_device", None, vp)
 _sig("rb_scene_device_bytes", C.c_int64, vp)
+_sig("rb_scene_layout_info", C.c_int, vp, c_int32_p, c_int32_p, c_float_p)
 _sig("rb_primary_hits", C.c_int, vp, C.c_int, C.c_int, c_double_p, vp, vp, vp)
 _sig("rb_get_render_opts", None, C.POINTER(RenderOpts))
 _sig("rb_set_render_opts", None, C.POINTER(RenderOpts))

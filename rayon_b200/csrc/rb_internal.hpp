@@ -44,6 +44,8 @@ struct DeviceScene {
   void *handle = nullptr;  // device pointer handed out as CudaScene::Scene*
   size_t bytes = 0;
   int ms = 3;
+  int layout_kind = 0, layout_leaf = 0;
+  float probe_ms = 0.0f;
 };
 
 // FP32 camera frame for the kernels (cast from the FP64 frame, as
@@ -61,6 +63,7 @@ void set_error(const std::string &msg);
 DeviceScene *lookup_scene(const void *handle);
 void build_quantized(HostLayout &L);
 FrameF frame_from(const double *fr, int w, int h);
+struct HostScene;
 rbd::Globals current_globals();
 rb_render_opts current_opts();
 

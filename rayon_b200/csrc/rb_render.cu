@@ -340,6 +340,8 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
        cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize(upload)");
   ds->bytes = bytes + 256;
   ds->ms = L.ms;
+  ds->layout_kind = L.use_bvh ? RB_LAYOUT_LEAF : RB_LAYOUT_LINEAR;
+  ds->layout_leaf = L.use_bvh ? hs.max_leaf : 0;
   if (!ok) {
     free_device_scene(ds);
     return nullptr;
@@ -347,6 +349,15 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
   std::lock_guard<std::mutex> lk(g_mu);
   g_scenes[ds->handle] = ds;
   return ds;
+}
+
+void unregister_and_free(DeviceScene *ds) {
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_scenes.erase(ds->handle);
+  }
+  cudaDeviceSynchronize();
+  free_device_scene(ds);
 }
 
 // ---------------------------------------------------------------------------
@@ -658,6 +669,159 @@ static void finish_display(unsigned char *out, size_t bytes) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Layout autotuner
+// ---------------------------------------------------------------------------
+// Candidate layouts are uploaded in turn and timed on a probe render whose
+// camera is derived from the scene's bounds (looking at the box centre from
+// 1.5 box diagonals away along (1, 0.6, 1.3)), 128 x 128 pixels, 4 samples,
+// so the choice needs no job: primary rays cover the scene and the bounces
+// stand in for secondary rays. The fastest candidate is kept.
+static float probe_ms(const DeviceScene *ds, const HostScene &hs, int depth, cudaStream_t st) {
+  double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+  for (const Geom &g : hs.geoms) {
+    lo[0] = std::min(lo[0], g.bmin.x); lo[1] = std::min(lo[1], g.bmin.y); lo[2] = std::min(lo[2], g.bmin.z);
+    hi[0] = std::max(hi[0], g.bmax.x); hi[1] = std::max(hi[1], g.bmax.y); hi[2] = std::max(hi[2], g.bmax.z);
+  }
+  // ignore huge ground primitives when sizing the view: clamp to the median extent
+  const V3 c((lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5);
+  double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                          (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  if (!(diag > 0) || diag > 1e6) diag = 10.0;
+  const V3 dir = unit(V3(1.0, 0.6, 1.3));
+  const V3 from = c + (1.5 * diag) * dir;
+  const int W = 128, H = 128;
+  double fr[21];
+  camera_frame(from, c, V3(0, 1, 0), 40.0, W, H, fr);
+  FrameF P = frame_from(fr, W, H);
+  P.samples = 4;
+  P.sample_base = 0;
+  P.max_depth = depth;
+  P.seed = 12345u;
+  float4 *acc = nullptr;
+  if (!cuda_ok(cudaMallocAsync((void **)&acc, (size_t)W * H * 32, st), "autotune buffer")) return 1e30f;
+  cudaMemsetAsync(acc, 0, (size_t)W * H * 32, st);
+  Globals G = current_globals();
+  G.nee = 0;
+  G.dof_enabled = 0;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  launch_render(ds, G, P, acc, acc + W * H, nullptr, nullptr, st);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 3; ++r) {
+    cudaEventRecord(a, st);
+    launch_render(ds, G, P, acc, acc + W * H, nullptr, nullptr, st);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFreeAsync(acc, st);
+  cudaStreamSynchronize(st);
+  return best;
+}
+
+// Decisions are cached per (device, scene fingerprint): re-uploading the same
+// scene (a renderer that rebuilds its device scene every frame) skips probing.
+struct TuneKey {
+  int dev;
+  uint64_t fp;
+  bool operator==(const TuneKey &o) const { return dev == o.dev && fp == o.fp; }
+};
+struct TuneKeyHash {
+  size_t operator()(const TuneKey &k) const { return (size_t)(k.fp ^ ((uint64_t)k.dev << 56)); }
+};
+static std::unordered_map<TuneKey, std::pair<bool, int>, TuneKeyHash> g_tune_cache;
+
+static uint64_t scene_fingerprint(const HostScene &hs) {
+  uint64_t h = 1469598103934665603ull;
+  auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+  mix(hs.geoms.size());
+  mix(hs.materials.size());
+  for (const Geom &g : hs.geoms) {
+    uint64_t b[6];
+    std::memcpy(&b[0], &g.bmin.x, 8); std::memcpy(&b[1], &g.bmin.y, 8); std::memcpy(&b[2], &g.bmin.z, 8);
+    std::memcpy(&b[3], &g.bmax.x, 8); std::memcpy(&b[4], &g.bmax.y, 8); std::memcpy(&b[5], &g.bmax.z, 8);
+    for (uint64_t v : b) mix(v);
+    mix((uint64_t)g.type | ((uint64_t)(uint32_t)g.material_id << 8));
+  }
+  return h;
+}
+
+DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cudaStream_t st) {
+  const int depth = o0.tune_depth > 0 ? o0.tune_depth : 8;
+  struct Cand { bool linear; int leaf; };
+  std::vector<Cand> cands;
+  const size_t n = hs.geoms.size();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const TuneKey key{dev, scene_fingerprint(hs)};
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      cands.push_back({it->second.first, it->second.second});
+      cached = true;
+    }
+  }
+  if (!cached) {
+    if (n <= 4096) cands.push_back({true, 0});
+    if (n > 0) {
+      if (n > (1u << 20)) cands.push_back({false, 1}), cands.push_back({false, 4});
+      else for (int L : {1, 2, 4, 8}) cands.push_back({false, L});
+    }
+  }
+  DeviceScene *best = nullptr;
+  float best_ms = 1e30f;
+  for (const Cand &c : cands) {
+    rb_upload_opts o = o0;
+    o.layout = RB_LAYOUT_AS_BUILT;
+    DeviceScene *ds = nullptr;
+    if (c.linear) {
+      o.use_bvh = 0;
+      ds = upload_scene(hs, o, st);
+    } else if (hs.use_bvh && hs.max_leaf == c.leaf && !hs.nodes.empty()) {
+      o.use_bvh = 1;
+      ds = upload_scene(hs, o, st);
+    } else {
+      HostScene copy = hs;
+      copy.build_bvh(c.leaf, 0);
+      o.use_bvh = 1;
+      ds = upload_scene(copy, o, st);
+    }
+    if (!ds) continue;
+    ds->layout_kind = c.linear ? RB_LAYOUT_LINEAR : RB_LAYOUT_LEAF;
+    ds->layout_leaf = c.leaf;
+    if (cands.size() == 1) {  // cached (or only) choice: no probing
+      best = ds;
+      break;
+    }
+    const float ms = probe_ms(ds, hs, depth, st);
+    ds->probe_ms = ms;
+    if (ms < best_ms) {
+      if (best) unregister_and_free(best);
+      best = ds;
+      best_ms = ms;
+    } else {
+      unregister_and_free(ds);
+    }
+  }
+  if (!best) {
+    set_error("rb_scene_upload: no layout could be uploaded");
+    return nullptr;
+  }
+  if (!cached) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_tune_cache[key] = {best->layout_kind == RB_LAYOUT_LINEAR, best->layout_leaf};
+  }
+  return best;
+}
+
 }  // namespace rb
 
 // ===========================================================================
@@ -877,8 +1041,37 @@ rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opt
   std::memset(&o, 0, sizeof o);
   o.use_bvh = 1;
   if (opts) o = *opts;
-  DeviceScene *ds = upload_scene(host_scene_of(s), o, static_cast<cudaStream_t>(stream));
+  const HostScene &hs = host_scene_of(s);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DeviceScene *ds = nullptr;
+  try {
+    if (o.layout == RB_LAYOUT_AUTOTUNE) {
+      ds = autotune_upload(hs, o, st);
+    } else if (o.layout == RB_LAYOUT_LINEAR) {
+      o.use_bvh = 0;
+      ds = upload_scene(hs, o, st);
+      if (ds) ds->layout_kind = RB_LAYOUT_LINEAR;
+    } else if (o.layout == RB_LAYOUT_LEAF && o.max_leaf >= 1 && o.max_leaf <= 32 && o.max_leaf != hs.max_leaf) {
+      HostScene copy = hs;
+      copy.build_bvh(o.max_leaf, 0);
+      ds = upload_scene(copy, o, st);
+    } else {
+      ds = upload_scene(hs, o, st);
+    }
+  } catch (const std::exception &e) {
+    set_error(std::string("rb_scene_upload: ") + e.what());
+    return nullptr;
+  }
   return ds ? static_cast<rb_cuda_scene *>(ds->handle) : nullptr;
+}
+
+int rb_scene_layout_info(const rb_cuda_scene *scene, int *kind, int *leaf, float *probe_ms) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) return RB_ERR_NOT_FOUND;
+  if (kind) *kind = ds->layout_kind;
+  if (leaf) *leaf = ds->layout_leaf;
+  if (probe_ms) *probe_ms = ds->probe_ms;
+  return RB_OK;
 }
 
 void rb_scene_free_device(rb_cuda_scene *scene) {

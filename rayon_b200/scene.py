@@ -114,7 +114,7 @@ class SceneDescription:
 
     def __del__(self) -> None:
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:
             lib.rb_scene_destroy(h)
             self._h = None
 
@@ -215,10 +215,16 @@ class SceneDescription:
         return list(arr[:n])
 
     # --- device --------------------------------------------------------------------
-    def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None) -> "DeviceScene":
+    def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None, layout: str = "as_built",
+               max_leaf: int = 0, tune_depth: int = 0) -> "DeviceScene":
+        """layout: "as_built" (the built BVH; bit-exact primary hits), "autotune"
+        (fastest of linear / leaf 1, 2, 4, 8 on a probe render), "linear", "leaf"."""
         o = UploadOpts()
         o.quantized_bvh = int(quantized)
         o.use_bvh = int(use_bvh)
+        o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3}[layout]
+        o.max_leaf = int(max_leaf)
+        o.tune_depth = int(tune_depth)
         h = lib.rb_scene_upload(self._h, C.byref(o), stream)
         if not h:
             raise RuntimeError(f"rb_scene_upload failed: {(lib.rb_last_error() or b'').decode()}")
@@ -234,6 +240,12 @@ class DeviceScene:
     @property
     def nbytes(self) -> int:
         return int(lib.rb_scene_device_bytes(self.handle))
+
+    @property
+    def layout(self) -> dict:
+        k, leaf, ms = C.c_int32(0), C.c_int32(0), C.c_float(0)
+        lib.rb_scene_layout_info(self.handle, C.byref(k), C.byref(leaf), C.byref(ms))
+        return {"kind": "linear" if k.value == 2 else "bvh", "leaf": leaf.value, "probe_ms": ms.value}
 
     def free(self) -> None:
         if self.handle:

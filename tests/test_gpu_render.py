@@ -154,3 +154,26 @@ def test_converged_image_rmse_vs_reference_cuda(cuda, name):
     # same expectation => the cross RMSE is the noise RMSE, up to sampling scatter
     assert err < 1.35 * noise + 1e-4, (err, noise)
     ds.free()
+
+
+@pytest.mark.parametrize("name", ["cornell", "one_weekend", "mixed_materials"])
+def test_autotuned_layout_renders_the_same(cuda, name):
+    spec, spp = _cases()[name]
+    w, h = spec.width, spec.height
+    sc = spec.to_scene()
+    sc.build_bvh()
+    fr = spec.camera.frame(w, h)
+    a_ds = sc.upload()
+    t_ds = sc.upload(layout="autotune", tune_depth=spec.depth)
+    info = t_ds.layout
+    assert info["kind"] in ("linear", "bvh") and info["probe_ms"] > 0
+    a = render.render_accumulate(a_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
+    b = render.render_accumulate(t_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
+    # same sample streams; layouts can only differ on exact-t ties
+    bad = (np.abs(a - b) > 1e-3 * (1 + np.abs(a)) * spp).any(axis=2)
+    assert bad.mean() < 0.01
+    # the decision is cached: a second upload reuses it without probing
+    t2 = sc.upload(layout="autotune", tune_depth=spec.depth)
+    assert t2.layout["kind"] == info["kind"] and t2.layout["leaf"] == info["leaf"]
+    for d in (a_ds, t_ds, t2):
+        d.free()
