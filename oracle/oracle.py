@@ -48,6 +48,7 @@ def lib():
         L.orc_scene_create.argtypes = [dp, C.c_int64, C.POINTER(MaterialDesc), C.c_int, dp, i32p, i32p, u8p, u8p,
                                        C.c_int64, C.c_int]
         L.orc_scene_destroy.argtypes = [C.c_void_p]
+        L.orc_scene_set_sdf.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
         L.orc_primary.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, i32p, dp, i64p, C.c_int]
         L.orc_render.argtypes = [C.c_void_p, C.c_int, C.c_int, dp, i32p, C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.POINTER(OrcGlobals), C.c_uint32, C.c_uint32, dp, C.c_int, i64p]
@@ -58,7 +59,8 @@ def lib():
 class OracleScene:
     """FP64 scene built from a SceneDescription whose BVH has been built."""
 
-    def __init__(self, sc, use_bvh: bool = True) -> None:
+    def __init__(self, sc, use_bvh: bool = True, sdf: tuple | None = None) -> None:
+        """sdf = (blend radius k, max steps, epsilon) for scenes with SDF primitives."""
         from rayon_b200._native import MaterialDesc
         L = lib()
         self.geoms = np.ascontiguousarray(sc.export_geometry())
@@ -71,6 +73,8 @@ class OracleScene:
                                     b.bounds.ctypes.data_as(dp), b.a.ctypes.data_as(i32p), b.b.ctypes.data_as(i32p),
                                     b.is_leaf.ctypes.data_as(u8p), b.split_axis.ctypes.data_as(u8p), n,
                                     b.root if use_bvh else -1)
+        if sdf is not None:
+            L.orc_scene_set_sdf(self.h, float(sdf[0]), int(sdf[1]), float(sdf[2]))
 
     def primary(self, frame: np.ndarray, w: int, h: int, threads: int = 0):
         ids = np.zeros(w * h, np.int32)

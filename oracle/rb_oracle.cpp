@@ -85,6 +85,13 @@ struct Light {
   double area, cdf;
 };
 
+struct SdfP {
+  int type, mat;
+  D3 pos;
+  double a, b, c, round, bound;
+  double R[9];  // world -> local
+};
+
 struct Scene {
   std::vector<Geom> g;
   std::vector<Mat> m;
@@ -92,6 +99,11 @@ struct Scene {
   std::vector<Light> lights;
   double light_area = 0;
   int root = -1;
+  std::vector<SdfP> sdf;        // SDF primitives in geometry (leaf) order
+  std::vector<int> sdf_of_geom; // geometry index -> sdf index or -1
+  double sdf_k = 0;
+  int sdf_steps = 256;
+  double sdf_eps = 1e-4;
 };
 
 struct Counters {
@@ -202,18 +214,160 @@ bool t_tri(const D3 &v0, const D3 &v1, const D3 &v2, const Ray &r, double tmin, 
 
 D3 gv(const Geom &g, int i) { return D3(g.p[i], g.p[i + 1], g.p[i + 2]); }
 
+// SDF distance functions (cpu_shapes/sdf.hpp:105-160; rounded box = box of
+// half extents minus the rounding radius, grown by it), evaluated in the
+// primitive's local frame.
+double sdf_eval1(const SdfP &q, const D3 &pw) {
+  const D3 d0 = pw - q.pos;
+  const D3 p(q.R[0] * d0.x + q.R[1] * d0.y + q.R[2] * d0.z, q.R[3] * d0.x + q.R[4] * d0.y + q.R[5] * d0.z,
+             q.R[6] * d0.x + q.R[7] * d0.y + q.R[8] * d0.z);
+  switch (q.type) {
+    case RB_SDF_SPHERE: return p.len() - q.a;
+    case RB_SDF_BOX:
+    case RB_SDF_ROUND_BOX: {
+      const D3 qq(std::fabs(p.x) - (q.a - q.round), std::fabs(p.y) - (q.b - q.round), std::fabs(p.z) - (q.c - q.round));
+      const double out = D3(std::fmax(qq.x, 0.0), std::fmax(qq.y, 0.0), std::fmax(qq.z, 0.0)).len();
+      const double in = std::fmin(std::fmax(qq.x, std::fmax(qq.y, qq.z)), 0.0);
+      return out + in - q.round;
+    }
+    case RB_SDF_TORUS: {
+      const double qx = std::sqrt(p.x * p.x + p.z * p.z) - q.a;
+      return std::sqrt(qx * qx + p.y * p.y) - q.b;
+    }
+    case RB_SDF_CAPSULE: {
+      const double hh = q.b * 0.5, y = std::fmin(std::fmax(p.y, -hh), hh);
+      return D3(p.x, p.y - y, p.z).len() - q.a;
+    }
+    default: return 1e30;
+  }
+}
+
+// polynomial smooth minimum (sdf.hpp:410-416)
+double smin_poly(double d1, double d2, double k) {
+  const double h = std::fmin(std::fmax(0.5 + 0.5 * (d2 - d1) / k, 0.0), 1.0);
+  return d2 * (1.0 - h) + d1 * h - k * h * (1.0 - h);
+}
+
+double inflated_radius(const Scene &S, const SdfP &q) { return q.bound * 1.0001 + S.sdf_k + 1e-3; }
+
+// one SDF primitive marched alone (hard union, blend radius 0)
+bool t_sdf_single(const Scene &S, const SdfP &q, const Ray &r, double tmin, double tmax, double &tt) {
+  double t0;
+  const double R = inflated_radius(S, q);
+  if (!t_sphere(q.pos, R, r, tmin, tmax, t0)) {
+    if ((r.o - q.pos).len2() > R * R) return false;
+    t0 = tmin;
+  }
+  const double il = 1.0 / r.d.len();
+  double t = t0;
+  for (int i = 0; i < S.sdf_steps; ++i) {
+    const double d = sdf_eval1(q, r.at(t));
+    if (d < S.sdf_eps) {
+      if (t >= tmin && t <= tmax) { tt = t; return true; }
+      return false;
+    }
+    t += d * il;
+    if (t > tmax) return false;
+  }
+  return false;
+}
+
 bool prim_t(const Scene &S, int i, const Ray &r, double tmin, double tmax, double &t) {
   const Geom &g = S.g[i];
   switch (g.type) {
     case RB_GEOM_SPHERE: case RB_GEOM_DISPLACED_SPHERE: return t_sphere(gv(g, 0), g.p[3], r, tmin, tmax, t);
     case RB_GEOM_RECTANGLE: return t_rect(gv(g, 0), gv(g, 3), gv(g, 6), r, tmin, tmax, t);
     case RB_GEOM_TRIANGLE: return t_tri(gv(g, 0), gv(g, 3), gv(g, 6), r, tmin, tmax, t);
+    case RB_GEOM_SDF_PRIMITIVE:
+      if (S.sdf_k > 0 || S.sdf_of_geom[i] < 0) return false;  // smooth field handled after traversal
+      return t_sdf_single(S, S.sdf[S.sdf_of_geom[i]], r, tmin, tmax, t);
     default: return false;
   }
 }
 
+// Smooth-union field of the SDF primitives whose inflated bounding spheres
+// overlap [tmin, tmax], folded in index order; sphere tracing on the field's
+// magnitude; normal by central differences (step 5e-4); material of the
+// nearest primitive.
+bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &tt, D3 &n, int &mat) {
+  std::vector<int> c;
+  for (int i = 0; i < (int)S.sdf.size(); ++i) {
+    const SdfP &q = S.sdf[i];
+    const D3 oc = r.o - q.pos;
+    const double R = inflated_radius(S, q);
+    const double a = dot(r.d, r.d), hb = dot(oc, r.d), cc = dot(oc, oc) - R * R;
+    const double disc = hb * hb - a * cc;
+    if (disc < 0) continue;
+    const double sq = std::sqrt(disc), t0 = (-hb - sq) / a, t1 = (-hb + sq) / a;
+    if (t1 >= tmin && t0 <= tmax && c.size() < 24) c.push_back(i);
+  }
+  if (c.empty()) return false;
+  auto field = [&](const D3 &p, int *nearest) {
+    double F = 1e30, best = 1e30;
+    for (size_t k = 0; k < c.size(); ++k) {
+      const double d = sdf_eval1(S.sdf[c[k]], p);
+      if (nearest && d < best) { best = d; *nearest = c[k]; }
+      F = k == 0 ? d : smin_poly(F, d, S.sdf_k);
+    }
+    return F;
+  };
+  const double il = 1.0 / r.d.len();
+  double t = tmin;
+  double f0 = field(r.at(t), nullptr);
+  for (int k = 0; k < 8 && std::fabs(f0) < 2.0 * S.sdf_eps; ++k) {
+    t += 2.0 * S.sdf_eps * il;
+    f0 = field(r.at(t), nullptr);
+  }
+  const double sgn = f0 < 0 ? -1.0 : 1.0;
+  for (int i = 0; i < S.sdf_steps; ++i) {
+    const D3 p = r.at(t);
+    const double F = sgn * field(p, nullptr);
+    if (F < S.sdf_eps) {
+      if (t > tmax) return false;
+      const double e = 5e-4;
+      const D3 gr(field(p + D3(e, 0, 0), nullptr) - field(p - D3(e, 0, 0), nullptr),
+                  field(p + D3(0, e, 0), nullptr) - field(p - D3(0, e, 0), nullptr),
+                  field(p + D3(0, 0, e), nullptr) - field(p - D3(0, 0, e), nullptr));
+      const double gl = gr.len();
+      n = gl > 0 ? gr / gl : D3(0, 1, 0);
+      int nearest = c[0];
+      field(p, &nearest);
+      mat = S.sdf[nearest].mat;
+      tt = t;
+      return true;
+    }
+    t += F * il;
+    if (t > tmax) return false;
+  }
+  return false;
+}
+
+int trace_bvh(const Scene &S, const Ray &r, double tmin, double tmax, double &tout, bool any, Counters &c);
+
+// Closest (or first) hit: BVH primitives, then the smooth SDF field up to
+// the closest primitive hit. A field hit returns -2 with its normal/material.
+struct FieldHit {
+  D3 n;
+  int mat = 0;
+};
+int trace(const Scene &S, const Ray &r, double tmin, double tmax, double &tout, bool any, Counters &c,
+          FieldHit *fh = nullptr) {
+  const int h = trace_bvh(S, r, tmin, tmax, tout, any, c);
+  if (S.sdf_k > 0 && !S.sdf.empty() && !(any && h >= 0)) {
+    double ts;
+    D3 n;
+    int mat;
+    if (sdf_field(S, r, tmin, h >= 0 ? tout : tmax, ts, n, mat)) {
+      tout = ts;
+      if (fh) { fh->n = n; fh->mat = mat; }
+      return -2;
+    }
+  }
+  return h;
+}
+
 // hit_scene: DFS with push (far, near) by the ray's sign on the split axis.
-int trace(const Scene &S, const Ray &r, double tmin, double tmax, double &tout, bool any, Counters &c) {
+int trace_bvh(const Scene &S, const Ray &r, double tmin, double tmax, double &tout, bool any, Counters &c) {
   double closest = tmax;
   int hit = -1;
   if (S.root < 0) {
@@ -288,6 +442,19 @@ Surf surface(const Scene &S, const Ray &r, int i, double t) {
     s.front = dot(r.d, n) < 0;
     s.n = s.front ? n : -n;
     s.tangent = norm(u);
+  } else if (g.type == RB_GEOM_SDF_PRIMITIVE) {
+    const SdfP &q = S.sdf[S.sdf_of_geom[i]];
+    const double e = S.sdf_eps;
+    const D3 gr(sdf_eval1(q, s.p + D3(e, 0, 0)) - sdf_eval1(q, s.p - D3(e, 0, 0)),
+                sdf_eval1(q, s.p + D3(0, e, 0)) - sdf_eval1(q, s.p - D3(0, e, 0)),
+                sdf_eval1(q, s.p + D3(0, 0, e)) - sdf_eval1(q, s.p - D3(0, 0, e)));
+    const D3 n = norm(gr);
+    s.front = dot(r.d, n) < 0;
+    s.n = s.front ? n : -n;
+    D3 tg = cross(D3(0, 1, 0), n);
+    if (tg.len2() < 1e-6) tg = D3(1, 0, 0);
+    s.tangent = norm(tg);
+    s.center = q.pos;
   } else {
     const D3 v0 = gv(g, 0), e1 = gv(g, 3) - v0, e2 = gv(g, 6) - v0;
     const D3 geo = norm(cross(e1, e2));
@@ -561,12 +728,26 @@ D3 radiance(const Scene &S, const Globals &G, Ray ray, uint32_t key, int depth, 
   for (int bounce = 0; bounce < depth; ++bounce) {
     ++c.segments;
     double t;
-    const int h = trace(S, ray, 0.001, 3.4028234663852886e38, t, false, c);
-    if (h < 0) {
+    FieldHit fh;
+    const int h = trace(S, ray, 0.001, 3.4028234663852886e38, t, false, c, &fh);
+    if (h == -1) {
       L = L + thr * sky(ray.d) * G.background;
       return L;
     }
-    const Surf s = surface(S, ray, h, t);
+    Surf s;
+    if (h == -2) {
+      s.p = ray.at(t) + (4.0 * S.sdf_eps) * fh.n * (dot(ray.d, fh.n) < 0 ? 1.0 : -1.0);
+      s.front = dot(ray.d, fh.n) < 0;
+      s.n = s.front ? fh.n : -fh.n;
+      D3 tg = cross(D3(0, 1, 0), fh.n);
+      if (tg.len2() < 1e-6) tg = D3(1, 0, 0);
+      s.tangent = norm(tg);
+      s.center = D3(0, 0, 0);
+      s.visible = true;
+      s.mat = fh.mat;
+    } else {
+      s = surface(S, ray, h, t);
+    }
     if (!s.visible && bounce == 0) {
       ray.o = s.p + ray.d * 0.01;
       continue;
@@ -599,7 +780,7 @@ D3 radiance(const Scene &S, const Globals &G, Ray ray, uint32_t key, int depth, 
             ++c.shadow;
             double ts;
             Ray sr{o.ray.o, wi};
-            if (trace(S, sr, 0.001, dist * (1 - 1e-4), ts, true, c) < 0) {
+            if (trace(S, sr, 0.001, dist * (1 - 1e-4), ts, true, c) == -1) {
               const double pl = d2 / (cl * S.light_area), pb = cs / PI;
               L = L + thr * o.att * Le * (cs / PI * mis2(pl, pb) / pl);
             }
@@ -673,6 +854,32 @@ void *orc_scene_create(const double *geoms, int64_t n, const rb_material_desc *m
     nd.axis = axis[i];
   }
   S->root = nnodes > 0 ? root : -1;
+  S->sdf_of_geom.assign(n, -1);
+  for (int64_t i = 0; i < n; ++i) {
+    const Geom &g = S->g[i];
+    if (g.type != RB_GEOM_SDF_PRIMITIVE) continue;
+    const int t = (int)g.p[0];
+    if (t != RB_SDF_SPHERE && t != RB_SDF_BOX && t != RB_SDF_ROUND_BOX && t != RB_SDF_TORUS && t != RB_SDF_CAPSULE)
+      continue;
+    SdfP q;
+    q.type = t;
+    q.mat = g.mat;
+    q.pos = gv(g, 1);
+    q.a = g.p[4]; q.b = g.p[5]; q.c = g.p[6];
+    q.round = t == RB_SDF_ROUND_BOX ? 0.2 * std::fmin(g.p[4], std::fmin(g.p[5], g.p[6])) : 0.0;
+    const double a = std::fabs(q.a), b = std::fabs(q.b), c = std::fabs(q.c);
+    q.bound = (t == RB_SDF_SPHERE) ? a : (t == RB_SDF_TORUS) ? a + b : (t == RB_SDF_CAPSULE) ? a + 0.5 * b
+                                                                                               : std::sqrt(a * a + b * b + c * c);
+    const double cx = std::cos(g.p[7]), sx = std::sin(g.p[7]), cy = std::cos(g.p[8]), sy = std::sin(g.p[8]);
+    const double cz = std::cos(g.p[9]), sz = std::sin(g.p[9]);
+    const double R[3][3] = {{cz * cy, cz * sy * sx - sz * cx, cz * sy * cx + sz * sx},
+                            {sz * cy, sz * sy * sx + cz * cx, sz * sy * cx - cz * sx},
+                            {-sy, cy * sx, cy * cx}};
+    for (int a2 = 0; a2 < 3; ++a2)
+      for (int b2 = 0; b2 < 3; ++b2) q.R[3 * a2 + b2] = R[b2][a2];
+    S->sdf_of_geom[i] = (int)S->sdf.size();
+    S->sdf.push_back(q);
+  }
   for (int64_t i = 0; i < n; ++i) {
     const Geom &g = S->g[i];
     if (g.mat < 0 || g.mat >= nmat || S->m[g.mat].kind != L_LIGHT) continue;
@@ -690,6 +897,14 @@ void *orc_scene_create(const double *geoms, int64_t n, const rb_material_desc *m
 }
 
 void orc_scene_destroy(void *s) { delete static_cast<Scene *>(s); }
+
+// Smooth-union radius, step limit and hit epsilon of the SDF primitives.
+void orc_scene_set_sdf(void *sp, double k, int steps, double eps) {
+  Scene &S = *static_cast<Scene *>(sp);
+  S.sdf_k = k;
+  S.sdf_steps = steps;
+  S.sdf_eps = eps;
+}
 
 // Pixel-centre primary hits; counters[0..1] += nodes visited, prims tested.
 void orc_primary(void *sp, int w, int h, const double *fr, int32_t *ids, double *tout, int64_t *counters, int threads) {

@@ -290,8 +290,30 @@ struct Builder {
 
 }  // namespace
 
+double sdf_bound_radius(const Geom &g) {
+  const double a = std::fabs(g.p[4]), b = std::fabs(g.p[5]), c = std::fabs(g.p[6]);
+  switch ((int)g.p[0]) {
+    case RB_SDF_SPHERE: return a;
+    case RB_SDF_BOX:
+    case RB_SDF_ROUND_BOX: return std::sqrt(a * a + b * b + c * c);
+    case RB_SDF_TORUS: return a + b;
+    case RB_SDF_CAPSULE: return a + 0.5 * b;
+    default: return std::max(a, std::max(b, c));
+  }
+}
+
 bool HostScene::build_bvh(int leaf, int threads) {
   nodes.clear();
+  // SDF primitives are bounded by their own sphere grown by the smooth-union
+  // radius (the reference's pos -/+ params box does not contain tori or
+  // capsules, and blended surfaces reach up to k further)
+  for (Geom &g : geoms)
+    if (g.type == RB_GEOM_SDF_PRIMITIVE) {
+      const double r = sdf_bound_radius(g) * 1.0001 + sdf.blend_k + 1e-3;
+      const V3 c(g.p[1], g.p[2], g.p[3]);
+      g.bmin = c - V3(r, r, r);
+      g.bmax = c + V3(r, r, r);
+    }
   if (geoms.empty()) {
     root = -1;
     return false;

@@ -88,6 +88,9 @@ class HostScene {
   bool build_bvh(int max_leaf, int threads);
 };
 
+// Radius of a sphere around an SDF primitive's position that contains it.
+double sdf_bound_radius(const Geom &g);
+
 // Camera frame (camera_base.hpp:76-99), FP64. out = 7 x 3 doubles.
 void camera_frame(const V3 &look_from, const V3 &look_at, const V3 &vup, double vfov, int w, int h,
                   double out[21]);

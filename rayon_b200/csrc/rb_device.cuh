@@ -256,9 +256,18 @@ __device__ __forceinline__ bool t_tri(const f3 &v0, const f3 &edge1, const f3 &e
 
 static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &r, float tmin, float tmax);
 
+// SDF primitives of a smooth-union scene (blend radius k > 0) are not hit one
+// by one: a ray collects the ones whose k-inflated bounding spheres it crosses
+// and the union field of those is sphere-traced after the traversal.
+#define RB_SDF_CAND 24
+struct SdfCand {
+  int n;
+  int idx[RB_SDF_CAND];
+};
+
 template <int MS>
 __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
-                                       float &t) {
+                                       float &t, SdfCand *cand = nullptr) {
   const float4 *p = S.prims + 3 * (size_t)i;
   const float4 a = __ldg(p);
   const float4 c = __ldg(p + 2);
@@ -271,6 +280,18 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
   if (kind == PK_RECT)
     return t_rect(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
   if (MS >= 3 && kind == PK_SDF) {
+    if (cand) {
+      // collect when the inflated bounding sphere overlaps [tmin, tmax]
+      const f3 oc = r.o - f3(a.x, a.y, a.z);
+      const float aa = dot(r.d, r.d), hb = dot(oc, r.d), cc = dot(oc, oc) - a.w * a.w;
+      const float disc = hb * hb - aa * cc;
+      if (disc >= 0.0f) {
+        const float sq = sqrtf(disc);
+        const float t0 = (-hb - sq) / aa, t1 = (-hb + sq) / aa;
+        if (t1 >= tmin && t0 <= tmax && cand->n < RB_SDF_CAND) cand->idx[cand->n++] = __float_as_int(__ldg(p + 1).x);
+      }
+      return false;
+    }
     const float ts = sdf_march_prim(S, i, r, tmin, tmax);
     if (ts >= 0.0f) { t = ts; return true; }
   }
@@ -318,13 +339,47 @@ struct Stack {
 
 struct HitInfo {
   float t;
-  int prim;
+  int prim;      // primitive, -1 miss, -2 the smooth SDF field
+  f3 sdf_n;      // field hit: outward normal and material
+  int sdf_mat;
 };
+
+static __device__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax, SdfCand &c,
+                                       float &t, f3 &n, int &mat);
 
 // Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
 template <bool ANY, int MS>
+__device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
+                                             uint32_t &overflow, SdfCand *cand);
+
+// Closest (or, with ANY, first) hit including the smooth SDF field.
+template <bool ANY, int MS>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {
+  if (MS >= 3 && S.sdf_k > 0.0f && S.num_sdf > 0) {
+    SdfCand cand;
+    cand.n = 0;
+    HitInfo h = trace_bvh<ANY, MS>(S, ray, tmin, tmax, st, overflow, &cand);
+    if (ANY && h.prim >= 0) return h;
+    if (cand.n > 0) {
+      float ts;
+      f3 n;
+      int mat;
+      if (sdf_field_march(S, ray, tmin, h.t, cand, ts, n, mat)) {
+        h.t = ts;
+        h.prim = -2;
+        h.sdf_n = n;
+        h.sdf_mat = mat;
+      }
+    }
+    return h;
+  }
+  return trace_bvh<ANY, MS>(S, ray, tmin, tmax, st, overflow, nullptr);
+}
+
+template <bool ANY, int MS>
+__device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
+                                             uint32_t &overflow, SdfCand *cand) {
   HitInfo h;
   h.t = tmax;
   h.prim = -1;
@@ -332,7 +387,7 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
   if (!S.use_bvh) {
     for (int i = 0; i < S.num_prims; ++i) {
       float t;
-      if (prim_t<MS>(S, i, ray, tmin, closest, t)) {
+      if (prim_t<MS>(S, i, ray, tmin, closest, t, cand)) {
         closest = t;
         h.t = t;
         h.prim = i;
@@ -353,7 +408,7 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
       const int first = leaf_first(cur), cnt = leaf_count(cur);
       for (int i = 0; i < cnt; ++i) {
         float t;
-        if (prim_t<MS>(S, first + i, ray, tmin, closest, t)) {
+        if (prim_t<MS>(S, first + i, ray, tmin, closest, t, cand)) {
           closest = t;
           h.t = t;
           h.prim = first + i;
@@ -434,6 +489,19 @@ static __device__ Surface sdf_surface(const SceneView &S, int prim, const Ray &r
 
 template <int MS>
 __device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, const HitInfo &h) {
+  if (MS >= 3 && h.prim == -2) {  // smooth SDF field; the point is lifted 4 eps off the surface
+    Surface s;
+    s.p = r.at(h.t) + (4.0f * S.sdf_eps) * h.sdf_n * (dot(r.d, h.sdf_n) < 0 ? 1.0f : -1.0f);
+    s.front = dot(r.d, h.sdf_n) < 0;
+    s.n = s.front ? h.sdf_n : f3(-h.sdf_n.x, -h.sdf_n.y, -h.sdf_n.z);
+    f3 tg = cross(f3(0.0f, 1.0f, 0.0f), h.sdf_n);
+    if (tg.length_squared() < 1e-6f) tg = f3(1.0f, 0.0f, 0.0f);
+    s.tangent = normalize(tg);
+    s.center = f3(0.0f, 0.0f, 0.0f);
+    s.visible = true;
+    s.mat = h.sdf_mat;
+    return s;
+  }
   const float4 *p = S.prims + 3 * (size_t)h.prim;
   const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
   const uint32_t tag = __float_as_uint(c.w);

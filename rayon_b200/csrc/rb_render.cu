@@ -171,16 +171,14 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
         q.material = g.material_id;
         q.px = (float)g.p[1]; q.py = (float)g.p[2]; q.pz = (float)g.p[3];
         q.a = (float)g.p[4]; q.b = (float)g.p[5]; q.c = (float)g.p[6];
-        double bound = 0.0;
-        if (t == RB_SDF_SPHERE) bound = g.p[4];
-        else if (t == RB_SDF_BOX) bound = std::sqrt(g.p[4] * g.p[4] + g.p[5] * g.p[5] + g.p[6] * g.p[6]);
-        else if (t == RB_SDF_ROUND_BOX) {
-          // rounded box: half extents in params, rounding radius = min half extent * 0.2
-          bound = std::sqrt(g.p[4] * g.p[4] + g.p[5] * g.p[5] + g.p[6] * g.p[6]);
-          q.round = (float)(0.2 * std::min(g.p[4], std::min(g.p[5], g.p[6])));
-        } else if (t == RB_SDF_TORUS) bound = g.p[4] + g.p[5];
-        else if (t == RB_SDF_CAPSULE) bound = g.p[4] + 0.5 * g.p[5];
-        else { kind = PK_NONE; break; }
+        if (t != RB_SDF_SPHERE && t != RB_SDF_BOX && t != RB_SDF_ROUND_BOX && t != RB_SDF_TORUS &&
+            t != RB_SDF_CAPSULE) {
+          kind = PK_NONE;
+          break;
+        }
+        const double bound = sdf_bound_radius(g);
+        // rounded box: half extents in params, rounding radius = 0.2 x the smallest half extent
+        if (t == RB_SDF_ROUND_BOX) q.round = (float)(0.2 * std::min(g.p[4], std::min(g.p[5], g.p[6])));
         float R[9];
         const double rr[3] = {g.p[7], g.p[8], g.p[9]};
         rot_matrix(rr, R);

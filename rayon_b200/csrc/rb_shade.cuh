@@ -484,6 +484,72 @@ __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
   return d2 * (1.0f - h) + d1 * h - k * h * (1.0f - h);
 }
 
+// Smooth-union field of the collected SDF primitives: polynomial smooth
+// minimum (sdf.hpp:410-416) folded in primitive-index order over the
+// candidates whose inflated spheres overlap [tmin, tmax]. Sphere tracing on
+// the field's magnitude (a ray that starts inside marches to the exit), at
+// most S.sdf_steps steps, hit below S.sdf_eps; outward normal by central
+// differences with a 5e-4 step; the material is that of the nearest primitive.
+#define RB_SDF_NORMAL_EPS 5e-4f
+__device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCand &c, const f3 &p, int *nearest) {
+  float F = 1e30f, best = 1e30f;
+  for (int i = 0; i < c.n; ++i) {
+    const float d = sdf_eval1(S.sdf[c.idx[i]], p);
+    if (nearest && d < best) {
+      best = d;
+      *nearest = c.idx[i];
+    }
+    F = (i == 0) ? d : smin_poly(F, d, S.sdf_k);
+  }
+  return F;
+}
+
+static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax,
+                                                    SdfCand &c, float &t_out, f3 &n_out, int &mat_out) {
+  // sort candidates by index (insertion sort) so the fold order is fixed
+  for (int i = 1; i < c.n; ++i) {
+    const int v = c.idx[i];
+    int j = i - 1;
+    while (j >= 0 && c.idx[j] > v) {
+      c.idx[j + 1] = c.idx[j];
+      --j;
+    }
+    c.idx[j + 1] = v;
+  }
+  const float inv_len = 1.0f / r.d.length();
+  float t = tmin;
+  // a ray that starts in the eps shell around the surface (a bounce off the
+  // field) first steps out of it, so the inside/outside decision is made
+  // where the field is clearly signed
+  float f0 = sdf_field_eval(S, c, r.at(t), nullptr);
+  for (int k = 0; k < 8 && fabsf(f0) < 2.0f * S.sdf_eps; ++k) {
+    t += 2.0f * S.sdf_eps * inv_len;
+    f0 = sdf_field_eval(S, c, r.at(t), nullptr);
+  }
+  const float sgn = f0 < 0.0f ? -1.0f : 1.0f;
+  for (int i = 0; i < S.sdf_steps; ++i) {
+    const f3 p = r.at(t);
+    const float F = sgn * sdf_field_eval(S, c, p, nullptr);
+    if (F < S.sdf_eps) {
+      if (t > tmax) return false;
+      const float e = RB_SDF_NORMAL_EPS;
+      const f3 g(sdf_field_eval(S, c, p + f3(e, 0, 0), nullptr) - sdf_field_eval(S, c, p - f3(e, 0, 0), nullptr),
+                 sdf_field_eval(S, c, p + f3(0, e, 0), nullptr) - sdf_field_eval(S, c, p - f3(0, e, 0), nullptr),
+                 sdf_field_eval(S, c, p + f3(0, 0, e), nullptr) - sdf_field_eval(S, c, p - f3(0, 0, e), nullptr));
+      const float gl = g.length();
+      n_out = gl > 0.0f ? g / gl : f3(0.0f, 1.0f, 0.0f);
+      int nearest = c.idx[0];
+      sdf_field_eval(S, c, p, &nearest);
+      mat_out = S.sdf[nearest].material;
+      t_out = t;
+      return true;
+    }
+    t += F * inv_len;
+    if (t > tmax) return false;
+  }
+  return false;
+}
+
 // Single hard-union SDF primitive marched on its own (closest-hit test through
 // the BVH); returns t or -1.
 static __device__ __noinline__ float sdf_march_prim(const SceneView &S, int prim, const Ray &r, float tmin, float tmax) {
