@@ -182,6 +182,7 @@ def main():
     ap.add_argument("--impl", default="rayon_b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the equal-RMSE and serving sections")
     ap.add_argument("--small", action="store_true",
                     help="profiling case for ncu: same frame at 16 spp, no e2e/baselines")
     args = ap.parse_args()
@@ -276,7 +277,11 @@ def main():
             e2e_times.append(time.perf_counter() - t0)
             h2d = ds.nbytes + w * h * 12
             d2h = 5 * w * h * 12
-        e2e_t = min(e2e_times) if world == 1 else max(e2e_times)
+        e2e_t = min(e2e_times)
+        if world > 1:  # the slowest rank bounds the job
+            tt = torch.tensor([e2e_t], device="cuda")
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            e2e_t = float(tt.item())
         e2e = {"value": world * paths / e2e_t / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_t,
                "path": "renderPixelsCUDAAccumulative x5 + scene upload (host float3 accumulation)"}
@@ -321,6 +326,13 @@ def main():
             res["cpu_baseline"] = {"unavailable": str(e)}
     res["fp32_issue_peak_tflops_at_clock"] = fp32_peak
     res["mean_radiance"] = mean_rad
+    if rank == 0 and world == 1 and not args.small and not args.no_extras:
+        for key, fn in (("equal_rmse", lambda: equal_rmse_section(t_ms, paths)),
+                        ("serving", lambda: serving_section())):
+            try:
+                res[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                res[key] = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(res))
     if world > 1:
@@ -350,6 +362,122 @@ def reference_cuda(spec, fr):
     return {"mpaths_s": paths / (best * 1e-3) / 1e6, "ms_per_frame": best,
             "e2e_mpaths_s": paths / secs / 1e6 if secs > 0 else None,
             "note": "reference renderAccKernel (sm_100a build of its sources, -maxrregcount 80, fast math)"}
+
+
+def serving_section(n_jobs: int = 40, rate: float = 50.0):
+    """The serving mix (scaled down from 2000 jobs): Poisson arrivals at `rate`
+    jobs/s over the one-weekend, Cornell, icosphere and SDF scenes, resolutions
+    from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform [16, 1024], orbit
+    angle U[0, 2pi). Plain = each job as its own per-frame launch, back to back;
+    served = the batched serving loop with real-time arrivals."""
+    import torch
+
+    from rayon_b200 import lib, render, scenes, serving
+    t0 = time.time()
+    specs = [scenes.one_weekend(), scenes.cornell(), scenes.icospheres(), scenes.sdf_field()]
+    dss = []
+    for sp in specs:
+        sc = sp.to_scene()
+        sc.build_bvh()
+        layout = "autotune" if sp.n < (1 << 20) else "as_built"
+        dss.append(sc.upload(layout=layout, tune_depth=sp.depth))
+    setup = time.time() - t0
+    mix = scenes.serving_mix(n_jobs, rate=rate, n_scenes=len(specs))
+    frames = [scenes.orbit(specs[j["scene"]].camera, j["angle"]).frame(j["width"], j["height"]) for j in mix]
+    paths = sum(j["width"] * j["height"] * j["spp"] for j in mix)
+    # plain per-job launches
+    torch.cuda.synchronize()
+    tp = time.time()
+    for j, fr in zip(mix, frames):
+        sp = specs[j["scene"]]
+        render.set_globals(background=sp.background, dof=sp.dof)
+        acc = torch.zeros((j["width"] * j["height"] * 2, 4), device="cuda")
+        frc = np.ascontiguousarray(fr)
+        lib.rb_render_accumulate(dss[j["scene"]].handle, j["width"], j["height"],
+                                 frc.ctypes.data_as(C.POINTER(C.c_double)), j["spp"], 0, sp.depth,
+                                 C.c_void_p(acc.data_ptr()), C.c_void_p(acc.data_ptr() + j["width"] * j["height"] * 16),
+                                 None, None)
+        torch.cuda.synchronize()
+    plain = time.time() - tp
+    render.set_globals()
+    srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
+    ids = [srv.add_scene(ds) for ds in dss]
+    reqs = [serving.job(ids[j["scene"]], fr, j["width"], j["height"], j["spp"], specs[j["scene"]].depth,
+                        background=specs[j["scene"]].background, dof=specs[j["scene"]].dof, seed=k, arrival=j["t"])
+            for k, (j, fr) in enumerate(zip(mix, frames))]
+    tb = time.time()
+    srv.run_trace(reqs, realtime=True)
+    wall = time.time() - tb
+    st = srv.stats()
+    srv.close()
+    for ds in dss:
+        ds.free()
+    return {"jobs": n_jobs, "arrival_rate_per_s": rate, "paths": paths,
+            "offered_gpaths_per_s": paths / mix[-1]["t"] / 1e9,
+            "plain_per_job_mpaths_s": paths / plain / 1e6,
+            "served_mpaths_s_wall": paths / wall / 1e6,
+            "served_mpaths_s_device": st.paths / st.device_seconds / 1e6 if st.device_seconds else None,
+            "p50_latency_s": st.p50_latency, "p99_latency_s": st.p99_latency, "mean_latency_s": st.mean_latency,
+            "iterations": st.iterations, "peak_device_bytes": st.peak_device_bytes, "setup_s": setup,
+            "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}
+
+
+def equal_rmse_section(full_ms_plain: float, full_paths: int):
+    """Estimator efficiency at equal RMSE against the FP64 oracle (Cornell box
+    at 64x64): RMSE of 64-spp renders with and without next-event estimation
+    against an FP64 oracle image at 4096 spp (NEE), combined with each
+    estimator's Mpaths/s on the full 512x512 frame."""
+    import torch
+
+    from oracle.oracle import Globals, OracleScene
+    from rayon_b200 import lib, render, scenes
+    spec = scenes.cornell(width=64, height=64)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload(layout="autotune", tune_depth=spec.depth)
+    fr = spec.camera.frame(64, 64)
+    t0 = time.time()
+    ref, _ = OracleScene(sc).render(fr, 64, 64, 4096, spec.depth, Globals(background=0.0, nee=True), seed=777)
+    oracle_s = time.time() - t0
+    ref = ref.reshape(64, 64, 3) / 4096
+    out = {}
+    for nee in (False, True):
+        errs = []
+        for k in range(4):
+            img = render.render_accumulate(ds, fr, 64, 64, 64, spec.depth, background=0.0, nee=nee,
+                                           sample_base=64 * k) / 64
+            errs.append(np.sqrt(((img - ref) ** 2).mean()))
+        out["rmse_nee" if nee else "rmse_plain"] = float(np.mean(errs))
+    ds.free()
+    # NEE throughput on the full frame
+    big = scenes.cornell()
+    scb = big.to_scene()
+    scb.build_bvh()
+    dsb = scb.upload(layout="autotune", tune_depth=big.depth)
+    frb = big.camera.frame(big.width, big.height)
+    with render.options(nee=True):
+        render.set_globals(background=0.0)
+        acc = torch.zeros((big.width * big.height * 2, 4), device="cuda")
+        frc = np.ascontiguousarray(frb)
+        args = (dsb.handle, big.width, big.height, frc.ctypes.data_as(C.POINTER(C.c_double)), big.spp, 0, big.depth,
+                C.c_void_p(acc.data_ptr()), C.c_void_p(acc.data_ptr() + big.width * big.height * 16), None, None)
+        lib.rb_render_accumulate(*args)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        lib.rb_render_accumulate(*args)
+        b.record()
+        torch.cuda.synchronize()
+        ms_nee = a.elapsed_time(b)
+        render.set_globals()
+    dsb.free()
+    mp_plain = full_paths / (full_ms_plain * 1e-3) / 1e6
+    mp_nee = full_paths / (ms_nee * 1e-3) / 1e6
+    out.update({"mpaths_s_plain": mp_plain, "mpaths_s_nee": mp_nee, "oracle_seconds": oracle_s,
+                "equal_rmse_speedup_nee": (mp_nee / mp_plain) * (out["rmse_plain"] / out["rmse_nee"]) ** 2,
+                "note": "RMSE of 64-spp 64x64 renders vs FP64 oracle at 4096 spp; speedup = throughput ratio x "
+                        "variance ratio (paths needed for equal RMSE)"})
+    return out
 
 
 if __name__ == "__main__":

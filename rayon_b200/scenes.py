@@ -282,3 +282,34 @@ def sdf_field(seed: int = 11, count: int = 256, width: int = 1280, height: int =
 
 
 CONFIGS = {"one_weekend": one_weekend, "cornell": cornell, "icospheres": icospheres, "sdf_field": sdf_field}
+
+
+def orbit(camera: Camera, angle: float) -> Camera:
+    """The camera rotated about the vertical axis through its target by `angle` radians."""
+    lf = np.array(camera.look_from, float)
+    la = np.array(camera.look_at, float)
+    d = lf - la
+    r = float(np.hypot(d[0], d[2]))
+    a0 = float(np.arctan2(d[2], d[0])) + angle
+    return Camera((la[0] + r * np.cos(a0), lf[1], la[2] + r * np.sin(a0)), camera.look_at, camera.vup, camera.vfov)
+
+
+SERVING_RESOLUTIONS = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+
+
+def serving_mix(n: int, rate: float = 50.0, n_scenes: int = 4, seed: int = 4, spp_range=(16, 1024)) -> list:
+    """The serving stream: Poisson arrivals at `rate` jobs/s; per job draw the
+    inter-arrival time, a resolution uniformly from SERVING_RESOLUTIONS, spp
+    log-uniform over spp_range, a scene index uniformly over n_scenes and an
+    orbit angle U[0, 2pi). Returns dicts (scene, width, height, spp, angle, t)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    t = 0.0
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate)
+        w, h = SERVING_RESOLUTIONS[int(rng.integers(0, len(SERVING_RESOLUTIONS)))]
+        spp = int(np.exp(rng.uniform(np.log(spp_range[0]), np.log(spp_range[1]))))
+        si = int(rng.integers(0, n_scenes))
+        ang = float(rng.uniform(0, 2 * np.pi))
+        jobs.append(dict(scene=si, width=w, height=h, spp=spp, angle=ang, t=t))
+    return jobs
