@@ -209,9 +209,9 @@ def main():
     paths = w * h * spp
     sc = spec.to_scene()
     sc.build_bvh()
-    ds = sc.upload(layout="autotune", tune_depth=depth)
-    layout = ds.layout
     fr = np.ascontiguousarray(spec.camera.frame(w, h), np.float64)
+    ds = sc.upload(layout="autotune", tune_depth=depth, probe=(fr, w, h))
+    layout = ds.layout
     frp = fr.ctypes.data_as(C.POINTER(C.c_double))
     render.set_globals(background=spec.background)
     stream = torch.cuda.current_stream()
@@ -270,7 +270,7 @@ def main():
         e2e_times = []
         for i in range(max(1, min(3, args.steps))):
             t0 = time.perf_counter()
-            ds2 = sc.upload(layout="autotune", tune_depth=depth)  # tuning decision cached per scene
+            ds2 = sc.upload(layout="autotune", tune_depth=depth, probe=(fr, w, h))  # decision cached per scene
             img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
             ds2.free()
             torch.cuda.synchronize()

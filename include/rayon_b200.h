@@ -215,13 +215,16 @@ typedef struct rb_upload_opts {
   int layout;          /* RB_LAYOUT_*: how the render kernels see the scene */
   int max_leaf;        /* RB_LAYOUT_LEAF: BVH leaf size to rebuild with */
   int tune_depth;      /* path depth of the autotuner's probe (0 = 8) */
-  int reserved[3];
+  int probe_width, probe_height;  /* frame size probe_frame was made for */
+  const double *probe_frame;      /* autotune on this camera (rb_camera_frame), or NULL */
 } rb_upload_opts;
 
 /* RB_LAYOUT_AS_BUILT: the scene's BVH as built (the reference's leaf-4 tree
  * from rb_scene_build_bvh: primary-hit ids bit-exact against the reference).
- * RB_LAYOUT_AUTOTUNE: time a probe render on each candidate layout (linear
- * scan for small scenes, BVH leaf sizes 1/2/4/8) and keep the fastest.
+ * RB_LAYOUT_AUTOTUNE: time a probe render (256 x 256 samples of probe_frame's
+ * view, 8 spp; without a frame, views from inside and outside the scene's box)
+ * on each candidate layout (linear scan for small scenes, BVH leaf sizes
+ * 1/2/4/8) and keep the fastest; decisions are cached per scene.
  * RB_LAYOUT_LINEAR: no BVH. RB_LAYOUT_LEAF: rebuild the BVH with max_leaf. */
 enum { RB_LAYOUT_AS_BUILT = 0, RB_LAYOUT_AUTOTUNE = 1, RB_LAYOUT_LINEAR = 2, RB_LAYOUT_LEAF = 3 };
 

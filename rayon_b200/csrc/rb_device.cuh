@@ -25,14 +25,14 @@ struct f3 {
   float x, y, z;
   __host__ __device__ __forceinline__ f3() {}
   __host__ __device__ __forceinline__ f3(float a, float b, float c) : x(a), y(b), z(c) {}
-  __device__ __forceinline__ f3 operator+(const f3 &o) const { return f3(x + o.x, y + o.y, z + o.z); }
-  __device__ __forceinline__ f3 operator-(const f3 &o) const { return f3(x - o.x, y - o.y, z - o.z); }
-  __device__ __forceinline__ f3 operator*(float t) const { return f3(x * t, y * t, z * t); }
-  __device__ __forceinline__ f3 operator*(const f3 &o) const { return f3(x * o.x, y * o.y, z * o.z); }
-  __device__ __forceinline__ f3 operator/(float t) const { return f3(x / t, y / t, z / t); }
-  __device__ __forceinline__ f3 operator-() const { return f3(-x, -y, -z); }
-  __device__ __forceinline__ float length() const { return sqrtf(x * x + y * y + z * z); }
-  __device__ __forceinline__ float length_squared() const { return x * x + y * y + z * z; }
+  __host__ __device__ __forceinline__ f3 operator+(const f3 &o) const { return f3(x + o.x, y + o.y, z + o.z); }
+  __host__ __device__ __forceinline__ f3 operator-(const f3 &o) const { return f3(x - o.x, y - o.y, z - o.z); }
+  __host__ __device__ __forceinline__ f3 operator*(float t) const { return f3(x * t, y * t, z * t); }
+  __host__ __device__ __forceinline__ f3 operator*(const f3 &o) const { return f3(x * o.x, y * o.y, z * o.z); }
+  __host__ __device__ __forceinline__ f3 operator/(float t) const { return f3(x / t, y / t, z / t); }
+  __host__ __device__ __forceinline__ f3 operator-() const { return f3(-x, -y, -z); }
+  __host__ __device__ __forceinline__ float length() const { return sqrtf(x * x + y * y + z * z); }
+  __host__ __device__ __forceinline__ float length_squared() const { return x * x + y * y + z * z; }
 };
 __device__ __forceinline__ f3 operator*(float t, const f3 &v) { return v * t; }
 __device__ __forceinline__ float dot(const f3 &a, const f3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }

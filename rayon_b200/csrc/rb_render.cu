@@ -670,32 +670,15 @@ static void finish_display(unsigned char *out, size_t bytes) {
 // ---------------------------------------------------------------------------
 // Layout autotuner
 // ---------------------------------------------------------------------------
-// Candidate layouts are uploaded in turn and timed on a probe render whose
-// camera is derived from the scene's bounds (looking at the box centre from
-// 1.5 box diagonals away along (1, 0.6, 1.3)), 128 x 128 pixels, 4 samples,
-// so the choice needs no job: primary rays cover the scene and the bounces
-// stand in for secondary rays. The fastest candidate is kept.
-static float probe_ms(const DeviceScene *ds, const HostScene &hs, int depth, cudaStream_t st) {
-  double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
-  for (const Geom &g : hs.geoms) {
-    lo[0] = std::min(lo[0], g.bmin.x); lo[1] = std::min(lo[1], g.bmin.y); lo[2] = std::min(lo[2], g.bmin.z);
-    hi[0] = std::max(hi[0], g.bmax.x); hi[1] = std::max(hi[1], g.bmax.y); hi[2] = std::max(hi[2], g.bmax.z);
-  }
-  // ignore huge ground primitives when sizing the view: clamp to the median extent
-  const V3 c((lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5);
-  double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                          (hi[2] - lo[2]) * (hi[2] - lo[2]));
-  if (!(diag > 0) || diag > 1e6) diag = 10.0;
-  const V3 dir = unit(V3(1.0, 0.6, 1.3));
-  const V3 from = c + (1.5 * diag) * dir;
-  const int W = 128, H = 128;
-  double fr[21];
-  camera_frame(from, c, V3(0, 1, 0), 40.0, W, H, fr);
-  FrameF P = frame_from(fr, W, H);
-  P.samples = 4;
-  P.sample_base = 0;
-  P.max_depth = depth;
-  P.seed = 12345u;
+// Candidate layouts are uploaded in turn and timed on a probe render of
+// 256 x 256 pixels at 8 samples: the caller's camera subsampled to that size
+// when given, otherwise two views of the scene's box (from its centre looking
+// along +x, and from 1.5 box diagonals outside looking at the centre), so
+// interior scenes and open scenes are both represented. The fastest
+// candidate is kept.
+static float probe_once(const DeviceScene *ds, const FrameF &P0, cudaStream_t st) {
+  FrameF P = P0;
+  const int W = P.width, H = P.height;
   float4 *acc = nullptr;
   if (!cuda_ok(cudaMallocAsync((void **)&acc, (size_t)W * H * 32, st), "autotune buffer")) return 1e30f;
   cudaMemsetAsync(acc, 0, (size_t)W * H * 32, st);
@@ -721,6 +704,47 @@ static float probe_ms(const DeviceScene *ds, const HostScene &hs, int depth, cud
   cudaFreeAsync(acc, st);
   cudaStreamSynchronize(st);
   return best;
+}
+
+static std::vector<FrameF> probe_frames(const HostScene &hs, const rb_upload_opts &o, int depth) {
+  std::vector<FrameF> out;
+  const int W = 256, H = 256;
+  auto finish = [&](FrameF P) {
+    P.samples = 8;
+    P.sample_base = 0;
+    P.max_depth = depth;
+    P.seed = 12345u;
+    return P;
+  };
+  if (o.probe_frame && o.probe_width > 0 && o.probe_height > 0) {
+    FrameF P = frame_from(o.probe_frame, W, H);
+    const float sx = (float)o.probe_width / W, sy = (float)o.probe_height / H;
+    P.du = P.du * sx;
+    P.dv = P.dv * sy;
+    out.push_back(finish(P));
+    return out;
+  }
+  double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+  for (const Geom &g : hs.geoms) {
+    lo[0] = std::min(lo[0], g.bmin.x); lo[1] = std::min(lo[1], g.bmin.y); lo[2] = std::min(lo[2], g.bmin.z);
+    hi[0] = std::max(hi[0], g.bmax.x); hi[1] = std::max(hi[1], g.bmax.y); hi[2] = std::max(hi[2], g.bmax.z);
+  }
+  const V3 c((lo[0] + hi[0]) * 0.5, (lo[1] + hi[1]) * 0.5, (lo[2] + hi[2]) * 0.5);
+  double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                          (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  if (!(diag > 0) || diag > 1e6) diag = 10.0;
+  double fr[21];
+  camera_frame(c, c + V3(1.0, 0.0, 0.0), V3(0, 1, 0), 70.0, W, H, fr);
+  out.push_back(finish(frame_from(fr, W, H)));
+  camera_frame(c + (1.5 * diag) * unit(V3(1.0, 0.6, 1.3)), c, V3(0, 1, 0), 40.0, W, H, fr);
+  out.push_back(finish(frame_from(fr, W, H)));
+  return out;
+}
+
+static float probe_ms(const DeviceScene *ds, const std::vector<FrameF> &frames, cudaStream_t st) {
+  float total = 0.f;
+  for (const FrameF &P : frames) total += probe_once(ds, P, st);
+  return total;
 }
 
 // Decisions are cached per (device, scene fingerprint): re-uploading the same
@@ -752,6 +776,7 @@ static uint64_t scene_fingerprint(const HostScene &hs) {
 
 DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cudaStream_t st) {
   const int depth = o0.tune_depth > 0 ? o0.tune_depth : 8;
+  const std::vector<FrameF> frames = probe_frames(hs, o0, depth);
   struct Cand { bool linear; int leaf; };
   std::vector<Cand> cands;
   const size_t n = hs.geoms.size();
@@ -799,7 +824,7 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
       best = ds;
       break;
     }
-    const float ms = probe_ms(ds, hs, depth, st);
+    const float ms = probe_ms(ds, frames, st);
     ds->probe_ms = ms;
     if (ms < best_ms) {
       if (best) unregister_and_free(best);

@@ -216,7 +216,7 @@ class SceneDescription:
 
     # --- device --------------------------------------------------------------------
     def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None, layout: str = "as_built",
-               max_leaf: int = 0, tune_depth: int = 0) -> "DeviceScene":
+               max_leaf: int = 0, tune_depth: int = 0, probe=None) -> "DeviceScene":
         """layout: "as_built" (the built BVH; bit-exact primary hits), "autotune"
         (fastest of linear / leaf 1, 2, 4, 8 on a probe render), "linear", "leaf"."""
         o = UploadOpts()
@@ -225,6 +225,11 @@ class SceneDescription:
         o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3}[layout]
         o.max_leaf = int(max_leaf)
         o.tune_depth = int(tune_depth)
+        keep = None
+        if probe is not None:  # (frame[21], width, height): autotune on this camera
+            keep = np.ascontiguousarray(probe[0], np.float64)
+            o.probe_frame = keep.ctypes.data_as(c_double_p)
+            o.probe_width, o.probe_height = int(probe[1]), int(probe[2])
         h = lib.rb_scene_upload(self._h, C.byref(o), stream)
         if not h:
             raise RuntimeError(f"rb_scene_upload failed: {(lib.rb_last_error() or b'').decode()}")
