@@ -46,6 +46,10 @@ struct __align__(16) BatchJob {
   int pad[3];
 };
 
+// Control blocks: [0] all jobs (frames), [1..8] one per launch group
+// (kernel class 1-4, plus 4 for the next-event-estimation variant).
+#define RB_GROUPS 9
+
 struct BatchCtl {
   unsigned long long next_task;
   unsigned long long total_tasks;
@@ -67,7 +71,7 @@ __device__ __forceinline__ int find_job(const BatchJob *__restrict__ jobs, int n
   return lo;
 }
 
-template <int MS, int MINB>
+template <int MS, int MINB, bool NEE>
 __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict__ jobs, BatchCtl *__restrict__ ctl) {
   extern __shared__ int2 smem[];
   jobs += ctl->job_offset;
@@ -152,7 +156,7 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
       }
       if (alive) {
         ++segs;
-        if (path_segment<true, MS>(J.S, J.G, st, ovf, ray, thr, L, bounce, prev_pdf, key, J.P.max_depth)) {
+        if (path_segment<NEE, MS>(J.S, J.G, st, ovf, ray, thr, L, bounce, prev_pdf, key, J.P.max_depth)) {
           kahan_add(sx, cx, L.x);
           kahan_add(sy, cy, L.y);
           kahan_add(sz, cz, L.z);
@@ -197,23 +201,53 @@ __global__ void k_batch_frames(const BatchJob *__restrict__ jobs, const BatchCtl
   o[3] = 255;
 }
 
-template <int MS>
+template <int MS, bool NEE>
 static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl) {
   const size_t sm = sizeof(int2) * RB_SHORT * 256;
   switch (minb) {
-    case 1: k_batch<MS, 1><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    case 3: k_batch<MS, 3><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    case 4: k_batch<MS, 4><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    default: k_batch<MS, 2><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 1: k_batch<MS, 1, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 3: k_batch<MS, 3, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    default: k_batch<MS, 2, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
   }
 }
 
-static void launch_batch(int ms, int minb, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms) {
+// One persistent launch for a class group; the next-event-estimation variant
+// only when a job of the group asks for it (it costs registers).
+static void launch_batch(int ms, int minb, bool nee, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms) {
   const int grid = sms * minb;  // persistent: exactly the resident blocks
-  if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE>(minb, grid, st, jobs, ctl);
-  else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC>(minb, grid, st, jobs, ctl);
-  else launch_batch_ms<RB_MS_FULL>(minb, grid, st, jobs, ctl);
+  if (nee) {
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, true>(minb, grid, st, jobs, ctl);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, true>(minb, grid, st, jobs, ctl);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, true>(minb, grid, st, jobs, ctl);
+    else launch_batch_ms<RB_MS_SDF, true>(minb, grid, st, jobs, ctl);
+  } else {
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, false>(minb, grid, st, jobs, ctl);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, false>(minb, grid, st, jobs, ctl);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, false>(minb, grid, st, jobs, ctl);
+    else launch_batch_ms<RB_MS_SDF, false>(minb, grid, st, jobs, ctl);
+  }
   g_launches++;
+}
+
+// Loads every batched-kernel variant up front so that lazy module loading
+// does not land inside a timed iteration.
+template <int MS>
+static void preload_ms() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_batch<MS, 1, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 2, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 3, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 1, true>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 2, true>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 3, true>);
+}
+static void preload_batch_kernels() {
+  preload_ms<RB_MS_DIFFUSE>();
+  preload_ms<RB_MS_CLASSIC>();
+  preload_ms<RB_MS_FULL>();
+  preload_ms<RB_MS_SDF>();
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_batch_frames);
 }
 
 // ---------------------------------------------------------------------------
@@ -335,7 +369,8 @@ static int server_step(Server &S) {
     Job &J = S.jobs[id];
     const double rem = (double)J.req.width * J.req.height * (J.req.spp - J.spp_done);
     const double age = tnow - J.t_arrival;
-    cand.push_back({id, 0, S.scenes[J.req.scene]->ms, rem / (1.0 + S.aging * age)});
+    // group key: kernel class, plus 4 when the job uses next-event estimation
+    cand.push_back({id, 0, S.scenes[J.req.scene]->ms + (J.req.nee ? 4 : 0), rem / (1.0 + S.aging * age)});
   }
   std::stable_sort(cand.begin(), cand.end(), [](const Plan &a, const Plan &b) { return a.prio < b.prio; });
   int64_t budget = S.o.paths_per_iteration;
@@ -358,8 +393,8 @@ static int server_step(Server &S) {
     return a.cls != b.cls ? a.cls < b.cls : a.spp > b.spp;
   });
   long long tb = 0;
-  std::memset(S.h_ctl, 0, sizeof(BatchCtl) * 4);
-  int jfirst[4] = {0, 0, 0, 0};
+  std::memset(S.h_ctl, 0, sizeof(BatchCtl) * RB_GROUPS);
+  int jfirst[RB_GROUPS] = {0};
   for (size_t k = 0; k < plan.size(); ++k) {
     Job &J = S.jobs[plan[k].id];
     const DeviceScene *ds = S.scenes[J.req.scene];
@@ -397,21 +432,23 @@ static int server_step(Server &S) {
     tb += (long long)J.req.width * J.req.height;
     C.total_tasks = (unsigned long long)tb;
   }
-  for (int c = 1; c <= 3; ++c) S.h_ctl[c].job_offset = jfirst[c];
+  for (int c = 1; c < RB_GROUPS; ++c) S.h_ctl[c].job_offset = jfirst[c];
   S.h_ctl[0].total_tasks = (unsigned long long)tb;             // all jobs (frames)
   S.h_ctl[0].njobs = (int)plan.size();
   const bool frames = S.o.frames_every > 0;
-  auto minb_of = [&](int cls) {
-    if (S.o.occupancy > 0) return S.o.occupancy;
-    return cls == RB_MS_DIFFUSE ? 3 : 2;
+  auto minb_of = [&](int grp) {
+    (void)grp;
+    return S.o.occupancy > 0 ? std::min(S.o.occupancy, 3) : 2;  // 2 resident blocks: tuned on B200
   };
-  auto kernels = [&](bool all_classes) {
-    for (int c = 1; c <= 3; ++c)
-      if (all_classes || S.h_ctl[c].njobs > 0)
-        launch_batch(c, minb_of(c), S.st, S.d_jobs, S.d_ctl + c, S.sms);
+  auto launch_group = [&](int grp) {
+    const int cls = grp > 4 ? grp - 4 : grp;
+    launch_batch(cls, minb_of(grp), grp > 4, S.st, S.d_jobs, S.d_ctl + grp, S.sms);
+  };
+  auto kernels = [&](bool all_groups) {
+    for (int c = 1; c < RB_GROUPS; ++c)
+      if (all_groups || S.h_ctl[c].njobs > 0) launch_group(c);
   };
   const long long frame_blocks_cap = (S.o.paths_per_iteration + 255) / 256 + 1;
-  cudaEventRecord(S.ev0, S.st);
   if (S.o.use_graph && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
     // One graph, reused every iteration: table and control blocks are copied
     // from pinned staging when the graph runs, the three class kernels are
@@ -423,19 +460,21 @@ static int server_step(Server &S) {
       cudaGraph_t g;
       if (!cuda_ok(cudaStreamBeginCapture(S.st, cudaStreamCaptureModeThreadLocal), "graph capture")) return RB_ERR_CUDA;
       cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * S.o.max_active_jobs, cudaMemcpyHostToDevice, S.st);
-      cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * 4, cudaMemcpyHostToDevice, S.st);
-      for (int c = 1; c <= 3; ++c) launch_batch(c, minb_of(c), S.st, S.d_jobs, S.d_ctl + c, S.sms);
+      cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
+      kernels(true);
       if (frames) k_batch_frames<<<(unsigned)frame_blocks_cap, 256, 0, S.st>>>(S.d_jobs, S.d_ctl);
       if (!cuda_ok(cudaStreamEndCapture(S.st, &g), "graph capture")) return RB_ERR_CUDA;
       if (!cuda_ok(cudaGraphInstantiate(&S.graph, g, 0), "graph instantiate")) return RB_ERR_CUDA;
       cudaGraphDestroy(g);
       S.graph_frames = (int)frames;
     }
+    cudaEventRecord(S.ev0, S.st);  // after any capture/instantiation: device time only
     if (!cuda_ok(cudaGraphLaunch(S.graph, S.st), "graph launch")) return RB_ERR_CUDA;
-    g_launches += 3 + (frames ? 1 : 0);
+    g_launches += (RB_GROUPS - 1) + (frames ? 1 : 0);
   } else {
+    cudaEventRecord(S.ev0, S.st);
     cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
-    cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * 4, cudaMemcpyHostToDevice, S.st);
+    cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
     kernels(false);
     if (frames) {
       k_batch_frames<<<(unsigned)((tb + 255) / 256), 256, 0, S.st>>>(S.d_jobs, S.d_ctl);
@@ -443,13 +482,13 @@ static int server_step(Server &S) {
     }
   }
   cudaEventRecord(S.ev1, S.st);
-  cudaMemcpyAsync(S.h_ctl, S.d_ctl, sizeof(BatchCtl) * 4, cudaMemcpyDeviceToHost, S.st);
+  cudaMemcpyAsync(S.h_ctl, S.d_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyDeviceToHost, S.st);
   if (!cuda_ok(cudaStreamSynchronize(S.st), "batched iteration")) return RB_ERR_CUDA;
   float ms_it = 0.f;
   cudaEventElapsedTime(&ms_it, S.ev0, S.ev1);
   S.stats.device_seconds += ms_it * 1e-3;
   S.stats.iterations++;
-  for (int c = 1; c <= 3; ++c) {
+  for (int c = 1; c < RB_GROUPS; ++c) {
     S.stats.paths += (int64_t)S.h_ctl[c].paths;
     S.stats.segments += (int64_t)S.h_ctl[c].segments;
   }
@@ -532,13 +571,14 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   cudaDeviceGetAttribute(&S.sms, cudaDevAttrMultiProcessorCount, dev);
   bool ok = cuda_ok(cudaMallocHost(&S.h_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server pinned jobs") &&
             cuda_ok(cudaMalloc(&S.d_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server jobs") &&
-            cuda_ok(cudaMallocHost(&S.h_ctl, sizeof(BatchCtl) * 4), "server pinned ctl") &&
-            cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * 4), "server ctl");
+            cuda_ok(cudaMallocHost(&S.h_ctl, sizeof(BatchCtl) * RB_GROUPS), "server pinned ctl") &&
+            cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * RB_GROUPS), "server ctl");
   if (!ok) {
     rb_server_destroy(r);
     return nullptr;
   }
   std::memset(S.h_jobs, 0, sizeof(BatchJob) * S.o.max_active_jobs);
+  preload_batch_kernels();
   cudaEventCreate(&S.ev0);
   cudaEventCreate(&S.ev1);
   std::memset(&S.stats, 0, sizeof S.stats);

@@ -279,7 +279,7 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
     return t_tri(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
   if (kind == PK_RECT)
     return t_rect(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
-  if (MS >= 3 && kind == PK_SDF) {
+  if (MS >= 4 && kind == PK_SDF) {
     if (cand) {
       // collect when the inflated bounding sphere overlaps [tmin, tmax]
       const f3 oc = r.o - f3(a.x, a.y, a.z);
@@ -356,7 +356,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
 template <bool ANY, int MS>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {
-  if (MS >= 3 && S.sdf_k > 0.0f && S.num_sdf > 0) {
+  if (MS >= 4 && S.sdf_k > 0.0f && S.num_sdf > 0) {
     SdfCand cand;
     cand.n = 0;
     HitInfo h = trace_bvh<ANY, MS>(S, ray, tmin, tmax, st, overflow, &cand);
@@ -489,7 +489,7 @@ static __device__ Surface sdf_surface(const SceneView &S, int prim, const Ray &r
 
 template <int MS>
 __device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, const HitInfo &h) {
-  if (MS >= 3 && h.prim == -2) {  // smooth SDF field; the point is lifted 4 eps off the surface
+  if (MS >= 4 && h.prim == -2) {  // smooth SDF field; the point is lifted 4 eps off the surface
     Surface s;
     s.p = r.at(h.t) + (4.0f * S.sdf_eps) * h.sdf_n * (dot(r.d, h.sdf_n) < 0 ? 1.0f : -1.0f);
     s.front = dot(r.d, h.sdf_n) < 0;
@@ -559,7 +559,7 @@ __device__ __forceinline__ Surface surface(const SceneView &S, const Ray &r, con
     g.visible = s.visible;
     g.mat = s.mat;
     return g;
-  } else if (MS >= 3) {
+  } else if (MS >= 4) {
     Surface g = sdf_surface(S, h.prim, r, h.t);
     g.visible = s.visible;
     g.mat = s.mat;

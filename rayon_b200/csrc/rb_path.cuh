@@ -44,7 +44,7 @@ __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &
                                              f3 &thr, f3 &L, int &bounce, float &prev_pdf, uint32_t key,
                                              int max_depth) {
   const HitInfo h = trace<false, MS>(S, ray, 0.001f, FLT_MAX, st, ovf);
-  if (h.prim < 0) {
+  if (h.prim == -1) {  // miss (-2 is a hit on the smooth SDF field)
     if (G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * G.background_intensity;
     return true;
   }
@@ -89,7 +89,7 @@ __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &
           sr.o = o;
           sr.d = wi;
           const HitInfo sh = trace<true, MS>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
-          if (sh.prim < 0) {
+          if (sh.prim == -1) {  // unoccluded
             const float pl = d2 / (cl * S.light_area);
             const float pb = cs * (1.0f / RB_PI);
             const float w = mis2(pl, pb);

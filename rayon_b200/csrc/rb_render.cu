@@ -230,8 +230,10 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     if (m.kind == L_MIRROR || m.kind == L_ROUGH_MIRROR || m.kind == L_GLASS) L.ms = std::max(L.ms, RB_MS_CLASSIC);
     if (m.kind == L_ANISO_METAL || m.kind == L_THIN_FILM || m.kind == L_CLEAR_COAT || m.pattern) L.ms = RB_MS_FULL;
   }
-  for (const auto &g : hs.geoms)
-    if (g.type == RB_GEOM_DISPLACED_SPHERE || g.type == RB_GEOM_SDF_PRIMITIVE) L.ms = RB_MS_FULL;
+  for (const auto &g : hs.geoms) {
+    if (g.type == RB_GEOM_DISPLACED_SPHERE) L.ms = std::max(L.ms, RB_MS_FULL);
+    if (g.type == RB_GEOM_SDF_PRIMITIVE) L.ms = RB_MS_SDF;
+  }
   if (!L.lights.empty()) L.lights.back().cdf = 3.0e38f;  // the last bin takes any rounding excess
 
   // BVH: interior nodes only, each holding its two children's boxes.
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t 
   Ray r;
   r.o = P.center;
   r.d = pc - P.center;
-  const HitInfo h = trace<false, RB_MS_FULL>(S, r, 0.001f, FLT_MAX, st, ovf);
+  const HitInfo h = trace<false, RB_MS_SDF>(S, r, 0.001f, FLT_MAX, st, ovf);
   const int pix = y * P.width + x;
   ids[pix] = h.prim;
   if (tout) tout[pix] = h.prim >= 0 ? h.t : -1.0f;
@@ -590,8 +592,8 @@ static int default_minb(int ms, bool nee) {
   return nee ? 1 : 2;
 }
 static void default_block(int ms, int &bx, int &by) {
-  bx = ms == RB_MS_FULL ? 32 : 16;
-  by = ms == RB_MS_FULL ? 4 : 8;
+  bx = ms >= RB_MS_FULL ? 32 : 16;
+  by = ms >= RB_MS_FULL ? 4 : 8;
 }
 
 template <bool NEE, int MS>
@@ -622,11 +624,13 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   if (G.nee) {
     if (ms == RB_MS_DIFFUSE) RB_LAUNCH(true, RB_MS_DIFFUSE);
     else if (ms == RB_MS_CLASSIC) RB_LAUNCH(true, RB_MS_CLASSIC);
-    else RB_LAUNCH(true, RB_MS_FULL);
+    else if (ms == RB_MS_FULL) RB_LAUNCH(true, RB_MS_FULL);
+    else RB_LAUNCH(true, RB_MS_SDF);
   } else {
     if (ms == RB_MS_DIFFUSE) RB_LAUNCH(false, RB_MS_DIFFUSE);
     else if (ms == RB_MS_CLASSIC) RB_LAUNCH(false, RB_MS_CLASSIC);
-    else RB_LAUNCH(false, RB_MS_FULL);
+    else if (ms == RB_MS_FULL) RB_LAUNCH(false, RB_MS_FULL);
+    else RB_LAUNCH(false, RB_MS_SDF);
   }
 #undef RB_LAUNCH
   g_launches++;

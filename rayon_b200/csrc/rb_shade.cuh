@@ -150,10 +150,12 @@ struct ScatterOut {
 //   RB_MS_DIFFUSE  Lambert, light, constant, normals
 //   RB_MS_CLASSIC  + mirror, rough mirror, glass
 //   RB_MS_FULL     + GGX conductor, thin film, clear coat, patterns,
-//                  displaced spheres and SDF primitives
+//                  displaced spheres
+//   RB_MS_SDF      + SDF primitives (hard union and the smooth-union field)
 #define RB_MS_DIFFUSE 1
 #define RB_MS_CLASSIC 2
 #define RB_MS_FULL 3
+#define RB_MS_SDF 4
 
 template <int MS>
 __device__ __forceinline__ ScatterOut scatter(const Globals &G, const DevMaterial &m, const Surface &s, const Ray &in,
