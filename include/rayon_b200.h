@@ -266,6 +266,18 @@ int rb_render_accumulate(const rb_cuda_scene *scene, int width, int height, cons
                          int samples_to_add, int sample_base, int max_depth, float *accum,
                          float *comp, uint64_t *counters, void *stream);
 
+/* Wavefront engine (an alternative to the per-pixel kernel of
+ * rb_render_accumulate): SoA ray/hit queues of queue_capacity paths (0 = 2^20),
+ * extend and shade kernels per bounce, warp-ballot compaction of surviving
+ * paths with in-place regeneration of ended ones, iterations replayed from a
+ * CUDA graph. Adds samples [sample_base, sample_base + samples) of every pixel
+ * to accum (DEVICE, w*h*4 doubles: FP64 sums x y z, pad) with FP64 atomics.
+ * counters (DEVICE, may be NULL): [segments, paths, stack overflows,
+ * iterations]. Same sample streams as rb_render_accumulate. */
+int rb_render_wavefront(const rb_cuda_scene *scene, int width, int height, const double frame[21],
+                        int samples, int sample_base, int max_depth, double *accum,
+                        int queue_capacity, uint64_t *counters, void *stream);
+
 /* Number of kernel launches this library has made (all entry points). */
 unsigned long long rb_launch_count(void);
 

@@ -141,6 +141,8 @@ _sig("rb_get_render_opts", None, C.POINTER(RenderOpts))
 _sig("rb_set_render_opts", None, C.POINTER(RenderOpts))
 _sig("rb_render_accumulate", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int,
      vp, vp, vp, vp)
+_sig("rb_render_wavefront", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp, C.c_int,
+     vp, vp)
 
 
 def last_error() -> str:

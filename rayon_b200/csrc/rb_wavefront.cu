@@ -1,0 +1,419 @@
+// Wavefront engine: the path tracer split into queue-connected kernels.
+//
+// Path state lives in structure-of-arrays queues of 16-byte elements (every
+// access is one 128-bit load or store, coalesced across the warp):
+//   o      float4 (origin xyz, prev. diffuse pdf)     d    float4 (direction xyz, -)
+//   thr    float4 (throughput xyz, -)                 L    float4 (radiance xyz, -)
+//   meta   int4   (pixel, sample, bounce, path key)   hit  float4 (t, prim, -, -)
+//   sn     float4 (SDF field normal xyz, material)    (written only on field hits)
+// One iteration is two launches over the live paths of queue A:
+//   extend: trace each ray to its closest hit (traversal only: few registers,
+//           high occupancy for latency hiding);
+//   shade:  surface, material scatter, emission, next-event estimation,
+//           Russian roulette; a path that ends adds its radiance to the
+//           pixel (FP64 atomics: order-independent sums) and its slot takes
+//           the next work item (path regeneration). Survivors and new paths
+//           are written compacted into queue B: each warp ballots its lanes
+//           that produce a path, one lane reserves the warp's range with one
+//           atomic, lanes write at their rank.
+// The queues then swap. Work items are sample-major (consecutive lanes take
+// consecutive pixels of the same sample) so primary rays of a warp are
+// coherent and the accumulation atomics of a warp hit distinct pixels. The
+// same counter-based sample streams as the per-frame kernel are used, so the
+// two engines agree path for path. Iterations are recorded once into a CUDA
+// graph (8 iterations per graph launch, ping-ponging the queues) and replayed
+// until the live count reaches zero.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+
+#include "rb_path.cuh"
+
+namespace rb {
+
+extern std::atomic<unsigned long long> g_launches;
+DeviceScene *lookup_scene(const void *handle);
+
+struct WfQueue {
+  float4 *o, *d, *thr, *L, *hit, *sn;
+  int4 *meta;
+};
+
+struct WfCtl {
+  unsigned long long next_path;   // next work item to generate
+  unsigned long long total_paths; // pixels * samples
+  int count[2];                   // live paths in queue 0 / 1
+  unsigned long long segments;
+  unsigned long long paths_done;
+  unsigned long long overflow;
+};
+
+struct WfParams {
+  SceneView S;
+  Globals G;
+  FrameF P;      // P.samples = samples per pixel of the launch, P.sample_base first sample
+  double *acc;   // w*h*4 doubles (xyz sums, pad)
+  WfCtl *ctl;
+};
+
+// Generates the camera ray of work item `item` into queue slot `k`.
+__device__ __forceinline__ void wf_emit_camera(const WfParams &W, const WfQueue &q, int k, unsigned long long item) {
+  const int npix = W.P.width * W.P.height;
+  const int pix = (int)(item % (unsigned long long)npix);
+  const int sample = (int)(item / (unsigned long long)npix);
+  const uint32_t key = rb_path_key(W.P.seed, W.P.salt, (uint32_t)pix, (uint32_t)(W.P.sample_base + sample));
+  const Ray r = camera_ray(W.P, W.G, pix % W.P.width, pix / W.P.width, key);
+  q.o[k] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+  q.d[k] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
+  q.thr[k] = make_float4(1.f, 1.f, 1.f, 0.f);
+  q.L[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+  q.meta[k] = make_int4(pix, sample, 0, (int)key);
+}
+
+// Initial fill of queue `qi` with min(capacity, total) fresh paths.
+__global__ void k_wf_fill(WfParams W, WfQueue q, int qi, int capacity) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long total = W.ctl->total_paths;
+  const unsigned long long n = total < (unsigned long long)capacity ? total : (unsigned long long)capacity;
+  if ((unsigned long long)k < n) wf_emit_camera(W, q, k, (unsigned long long)k);
+  if (k == 0) {
+    W.ctl->count[qi] = (int)n;
+    W.ctl->next_path = n;
+  }
+}
+
+template <int MS>
+__global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi) {
+  extern __shared__ int2 smem[];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= W.ctl->count[qi]) return;
+  Stack st;
+  st.sh = smem + threadIdx.x;
+  st.stride = blockDim.x;
+  uint32_t ovf = 0;
+  const float4 o = q.o[k], d = q.d[k];
+  Ray r;
+  r.o = f3(o.x, o.y, o.z);
+  r.d = f3(d.x, d.y, d.z);
+  const HitInfo h = trace<false, MS>(W.S, r, 0.001f, FLT_MAX, st, ovf);
+  q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
+  if (MS >= RB_MS_SDF && h.prim == -2) q.sn[k] = make_float4(h.sdf_n.x, h.sdf_n.y, h.sdf_n.z, __int_as_float(h.sdf_mat));
+  if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
+}
+
+template <int MS, bool NEE>
+__global__ void __launch_bounds__(256) k_wf_shade(WfParams W, WfQueue in, WfQueue out, int qi) {
+  extern __shared__ int2 smem[];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int n_in = W.ctl->count[qi];
+  bool have_out = false;
+  // outgoing path, held in registers until the warp's range is reserved
+  float4 no = make_float4(0, 0, 0, 0), nd = no, nthr = no, nL = no;
+  int4 nmeta = make_int4(0, 0, 0, 0);
+  bool regenerate = false;
+  if (k < n_in) {
+    Stack st;
+    st.sh = smem + threadIdx.x;
+    st.stride = blockDim.x;
+    uint32_t ovf = 0;
+    const float4 o = in.o[k], d = in.d[k], th = in.thr[k], Lv = in.L[k], hv = in.hit[k];
+    const int4 m = in.meta[k];
+    Ray ray;
+    ray.o = f3(o.x, o.y, o.z);
+    ray.d = f3(d.x, d.y, d.z);
+    f3 thr(th.x, th.y, th.z), L(Lv.x, Lv.y, Lv.z);
+    float prev_pdf = o.w;
+    int bounce = m.z;
+    const uint32_t key = (uint32_t)m.w;
+    HitInfo h;
+    h.t = hv.x;
+    h.prim = __float_as_int(hv.y);
+    if (MS >= RB_MS_SDF && h.prim == -2) {
+      const float4 s = in.sn[k];
+      h.sdf_n = f3(s.x, s.y, s.z);
+      h.sdf_mat = __float_as_int(s.w);
+    }
+    // shade with the precomputed hit (path_segment's body after its trace)
+    bool ended = false;
+    if (h.prim == -1) {
+      if (W.G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * W.G.background_intensity;
+      ended = true;
+    } else {
+      const Surface sf = surface<MS>(W.S, ray, h);
+      if (!sf.visible && bounce == 0) {
+        ray.o = sf.p + ray.d * 0.01f;
+        ended = ++bounce >= W.P.max_depth;
+      } else if (sf.mat >= W.S.num_mats) {
+        ended = true;
+      } else {
+        const DevMaterial &mt = W.S.mats[sf.mat];
+        const ScatterOut so = scatter<MS>(W.G, mt, sf, ray, key, bounce);
+        if (so.emit.length_squared() > 0.0f) {
+          float wgt = 1.0f;
+          if (NEE && W.G.nee && prev_pdf > 0.0f && mt.kind == L_LIGHT && W.S.num_lights > 0) {
+            const float dl = h.t * ray.d.length();
+            const float cl = fabsf(dot(sf.n, normalize(ray.d)));
+            const float pl = cl > 0.0f ? dl * dl / (cl * W.S.light_area) : 0.0f;
+            wgt = mis2(prev_pdf, pl);
+          }
+          L = L + thr * so.emit * wgt;
+        }
+        if (!so.scattered) {
+          ended = true;
+        } else {
+          if (NEE && W.G.nee) {
+            prev_pdf = 0.0f;
+            if (mt.kind == L_LAMBERTIAN && bounce + 1 < W.P.max_depth && W.S.num_lights > 0) {
+              LightSample ls;
+              const uint32_t dl = rb_vdim(bounce, RB_SLOT_LIGHT);
+              if (sample_light(W.S, W.G, rb_draw(key, dl), rb_draw(key, dl + 1), rb_draw(key, dl + 2), ls)) {
+                const f3 dv = ls.p - so.ray.o;
+                const float d2 = dv.length_squared();
+                const float dist = sqrtf(d2);
+                const f3 wi = dv / dist;
+                const float cs = dot(normalize(sf.n), wi);
+                const float cl = fabsf(dot(ls.n, wi));
+                if (cs > 0.0f && cl > 0.0f) {
+                  Ray sr;
+                  sr.o = so.ray.o;
+                  sr.d = wi;
+                  const HitInfo sh = trace<true, MS>(W.S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
+                  if (sh.prim == -1) {
+                    const float pl = d2 / (cl * W.S.light_area);
+                    const float pb = cs * (1.0f / RB_PI);
+                    L = L + thr * so.att * ls.Le * (cs * (1.0f / RB_PI) * mis2(pl, pb) / pl);
+                  }
+                }
+              }
+              prev_pdf = so.pdf;
+            }
+          }
+          thr = thr * so.att;
+          if (bounce > 0) {
+            const float sp = fminf(fmaxf(thr.x, fmaxf(thr.y, thr.z)), 0.95f);
+            if (rb_draw(key, rb_vdim(bounce, RB_SLOT_RR)) > sp) ended = true;
+            else thr = thr / sp;
+          }
+          if (!ended) {
+            ray = so.ray;
+            ended = ++bounce >= W.P.max_depth;
+          }
+        }
+      }
+    }
+    if (ended) {
+      double *a = W.acc + 4 * (size_t)m.x;
+      atomicAdd(a, (double)L.x);
+      atomicAdd(a + 1, (double)L.y);
+      atomicAdd(a + 2, (double)L.z);
+      regenerate = true;
+    } else {
+      have_out = true;
+      no = make_float4(ray.o.x, ray.o.y, ray.o.z, prev_pdf);
+      nd = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
+      nthr = make_float4(thr.x, thr.y, thr.z, 0.0f);
+      nL = make_float4(L.x, L.y, L.z, 0.0f);
+      nmeta = make_int4(m.x, m.y, bounce, m.w);
+    }
+    if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
+  }
+  // regeneration: ended paths claim the next work items (one atomic per warp)
+  const unsigned rmask = __ballot_sync(0xffffffffu, regenerate);
+  unsigned long long item = ~0ull;
+  if (rmask) {
+    unsigned long long base = 0;
+    const int leader = __ffs(rmask) - 1;
+    if (lane == leader) base = atomicAdd(&W.ctl->next_path, (unsigned long long)__popc(rmask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (regenerate) {
+      item = base + __popc(rmask & ((1u << lane) - 1u));
+      if (item >= W.ctl->total_paths) item = ~0ull;
+    }
+    if (lane == leader) atomicAdd(&W.ctl->paths_done, (unsigned long long)__popc(rmask));
+  }
+  const bool emits = have_out || item != ~0ull;
+  // compaction into the output queue (one atomic per warp)
+  const unsigned omask = __ballot_sync(0xffffffffu, emits);
+  if (omask) {
+    int base = 0;
+    const int leader = __ffs(omask) - 1;
+    if (lane == leader) base = atomicAdd(&W.ctl->count[qi ^ 1], __popc(omask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    const int slot = base + __popc(omask & ((1u << lane) - 1u));
+    if (have_out) {
+      out.o[slot] = no;
+      out.d[slot] = nd;
+      out.thr[slot] = nthr;
+      out.L[slot] = nL;
+      out.meta[slot] = nmeta;
+    } else if (emits) {
+      wf_emit_camera(W, out, slot, item);
+    }
+  }
+  const unsigned long long segs = (k < n_in) ? 1ull : 0ull;
+  unsigned long long s = segs;
+  for (int o2 = 16; o2 > 0; o2 >>= 1) s += __shfl_down_sync(0xffffffffu, s, o2);
+  if (lane == 0 && s) atomicAdd(&W.ctl->segments, s);
+}
+
+// Resets the live count of the queue the next shade writes into.
+__global__ void k_wf_reset(WfCtl *ctl, int qi) { ctl->count[qi] = 0; }
+
+struct WfEngine {
+  int capacity = 0;
+  WfQueue q[2];
+  WfCtl *ctl = nullptr;
+  WfCtl *h_ctl = nullptr;
+  cudaStream_t st = nullptr;
+};
+
+static void wf_free(WfEngine &E) {
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(E.q[i].o); cudaFree(E.q[i].d); cudaFree(E.q[i].thr); cudaFree(E.q[i].L);
+    cudaFree(E.q[i].hit); cudaFree(E.q[i].sn); cudaFree(E.q[i].meta);
+  }
+  cudaFree(E.ctl);
+  cudaFreeHost(E.h_ctl);
+}
+
+static bool wf_alloc(WfEngine &E, int capacity) {
+  std::memset(&E.q, 0, sizeof E.q);
+  E.capacity = capacity;
+  bool ok = true;
+  for (int i = 0; i < 2 && ok; ++i) {
+    ok = cuda_ok(cudaMalloc(&E.q[i].o, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].d, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].thr, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].L, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].hit, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].sn, sizeof(float4) * capacity), "wavefront queue") &&
+         cuda_ok(cudaMalloc(&E.q[i].meta, sizeof(int4) * capacity), "wavefront queue");
+  }
+  ok = ok && cuda_ok(cudaMalloc(&E.ctl, sizeof(WfCtl)), "wavefront ctl") &&
+       cuda_ok(cudaMallocHost(&E.h_ctl, sizeof(WfCtl)), "wavefront ctl");
+  return ok;
+}
+
+template <int MS, bool NEE>
+static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, cudaStream_t st) {
+  const size_t sm = sizeof(int2) * RB_SHORT * 256;
+  k_wf_reset<<<1, 1, 0, st>>>(E.ctl, qi ^ 1);
+  k_wf_extend<MS><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
+  k_wf_shade<MS, NEE><<<grid, 256, sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
+}
+
+template <int MS, bool NEE>
+static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
+  const int grid = (E.capacity + 255) / 256;
+  k_wf_fill<<<grid, 256, 0, st>>>(W, E.q[0], 0, E.capacity);
+  g_launches++;
+  // eight iterations per graph (queues 0->1->0 ...), replayed until empty
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  if (!cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "wavefront capture")) return RB_ERR_CUDA;
+  for (int i = 0; i < 8; ++i) wf_iteration<MS, NEE>(W, E, i & 1, grid, st);
+  const cudaError_t ec = cudaStreamEndCapture(st, &g);  // always end the capture, also after an error
+  if (!cuda_ok(ec, "wavefront capture") || !g) return RB_ERR_CUDA;
+  const bool inst = cuda_ok(cudaGraphInstantiate(&ge, g, 0), "wavefront graph");
+  cudaGraphDestroy(g);
+  if (!inst) return RB_ERR_CUDA;
+  int it = 0;
+  for (int guard = 0; guard < 1 << 20; ++guard) {
+    cudaGraphLaunch(ge, st);
+    g_launches += 24;
+    it += 8;
+    cudaMemcpyAsync(E.h_ctl, E.ctl, sizeof(WfCtl), cudaMemcpyDeviceToHost, st);
+    if (!cuda_ok(cudaStreamSynchronize(st), "wavefront iteration")) {
+      cudaGraphExecDestroy(ge);
+      return RB_ERR_CUDA;
+    }
+    if (E.h_ctl->count[0] == 0) break;  // eight iterations end in queue 0
+  }
+  cudaGraphExecDestroy(ge);
+  if (iterations) *iterations = it;
+  return RB_OK;
+}
+
+}  // namespace rb
+
+using namespace rb;
+
+extern "C" int rb_render_wavefront(const rb_cuda_scene *scene, int width, int height, const double frame[21],
+                                   int samples, int sample_base, int max_depth, double *accum, int queue_capacity,
+                                   uint64_t *counters, void *stream) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_render_wavefront: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  if (width <= 0 || height <= 0 || !frame || !accum || samples < 0 || max_depth < 0 || sample_base < 0) {
+    set_error("rb_render_wavefront: invalid argument");
+    return RB_ERR_INVALID_ARG;
+  }
+  if (samples == 0 || max_depth == 0) return RB_OK;
+  // The engine records its iterations into a CUDA graph, which needs a
+  // capturable stream: it runs on a private non-blocking stream ordered after
+  // the caller's stream on entry and before it on return.
+  cudaStream_t caller = static_cast<cudaStream_t>(stream);
+  static thread_local cudaStream_t priv[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return RB_ERR_UNSUPPORTED;
+  if (!priv[dev] && !cuda_ok(cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking), "wavefront stream"))
+    return RB_ERR_CUDA;
+  cudaStream_t st = priv[dev];
+  cudaEvent_t fence;
+  cudaEventCreateWithFlags(&fence, cudaEventDisableTiming);
+  cudaEventRecord(fence, caller);
+  cudaStreamWaitEvent(st, fence, 0);
+  // queues are kept per (device, capacity) between calls: a render loop pays
+  // for their allocation once (2 x 7 arrays of capacity x 16 B)
+  const int cap = queue_capacity > 0 ? queue_capacity : (1 << 20);
+  static thread_local WfEngine cached[64];
+  WfEngine &E = cached[dev];
+  if (E.capacity != cap) {
+    if (E.capacity) wf_free(E);
+    E.capacity = 0;
+    if (!wf_alloc(E, cap)) {
+      wf_free(E);
+      E.capacity = 0;
+      return RB_ERR_OUT_OF_MEMORY;
+    }
+  }
+  WfParams W;
+  std::memset(&W, 0, sizeof W);
+  W.S = ds->view;
+  W.G = current_globals();
+  W.P = frame_from(frame, width, height);
+  W.P.samples = samples;
+  W.P.sample_base = sample_base;
+  W.P.max_depth = max_depth;
+  W.P.seed = current_opts().seed;
+  W.P.salt = 0;
+  W.acc = accum;
+  W.ctl = E.ctl;
+  WfCtl init;
+  std::memset(&init, 0, sizeof init);
+  init.total_paths = (unsigned long long)width * height * samples;
+  cudaMemcpyAsync(E.ctl, &init, sizeof init, cudaMemcpyHostToDevice, st);
+  int it = 0, rc;
+  const bool nee = W.G.nee != 0;
+  switch (ds->ms) {
+    case RB_MS_DIFFUSE: rc = nee ? wf_run<RB_MS_DIFFUSE, true>(W, E, st, &it) : wf_run<RB_MS_DIFFUSE, false>(W, E, st, &it); break;
+    case RB_MS_CLASSIC: rc = nee ? wf_run<RB_MS_CLASSIC, true>(W, E, st, &it) : wf_run<RB_MS_CLASSIC, false>(W, E, st, &it); break;
+    case RB_MS_FULL: rc = nee ? wf_run<RB_MS_FULL, true>(W, E, st, &it) : wf_run<RB_MS_FULL, false>(W, E, st, &it); break;
+    default: rc = nee ? wf_run<RB_MS_SDF, true>(W, E, st, &it) : wf_run<RB_MS_SDF, false>(W, E, st, &it); break;
+  }
+  if (rc == RB_OK && counters) {
+    uint64_t c[4] = {E.h_ctl->segments, E.h_ctl->paths_done, E.h_ctl->overflow, (uint64_t)it};
+    cudaMemcpyAsync(counters, c, sizeof c, cudaMemcpyHostToDevice, st);
+  }
+  cudaEventRecord(fence, st);
+  cudaStreamWaitEvent(caller, fence, 0);
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(fence);
+  return rc;
+}

@@ -177,3 +177,23 @@ def test_autotuned_layout_renders_the_same(cuda, name):
     assert t2.layout["kind"] == info["kind"] and t2.layout["leaf"] == info["leaf"]
     for d in (a_ds, t_ds, t2):
         d.free()
+
+
+@pytest.mark.parametrize("name", ["cornell", "mixed_materials", "one_weekend", "small_icospheres"])
+@pytest.mark.parametrize("nee", [False, True])
+def test_wavefront_engine_paired_with_per_pixel_kernel(cuda, name, nee):
+    spec, spp = _cases()[name]
+    w, h = spec.width, spec.height
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = spec.camera.frame(w, h)
+    a = render.render_accumulate(ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof, nee=nee)
+    # a small queue forces many regeneration/compaction rounds
+    b, cnt = render.render_wavefront(ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof,
+                                     nee=nee, queue_capacity=4096, counters=True)
+    assert int(cnt[1]) == w * h * spp  # every path accounted for exactly once
+    bad = (np.abs(a - b) > 1e-3 * (1 + np.abs(a)) * spp).any(axis=2)
+    assert bad.mean() < 0.01, bad.mean()
+    np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=1e-2, atol=1e-4)
+    ds.free()
