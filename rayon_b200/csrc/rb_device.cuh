@@ -348,18 +348,20 @@ static __device__ bool sdf_field_march(const SceneView &S, const Ray &r, float t
                                        float &t, f3 &n, int &mat);
 
 // Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
-template <bool ANY, int MS>
+template <bool ANY, int MS, bool SPEC>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                              uint32_t &overflow, SdfCand *cand);
 
-// Closest (or, with ANY, first) hit including the smooth SDF field.
-template <bool ANY, int MS>
+// Closest (or, with ANY, first) hit including the smooth SDF field. SPEC
+// selects the speculative while-while traversal (render kernels); without it
+// the traversal visits nodes and primitives in the reference's exact order.
+template <bool ANY, int MS, bool SPEC = false>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {
   if (MS >= 4 && S.sdf_k > 0.0f && S.num_sdf > 0) {
     SdfCand cand;
     cand.n = 0;
-    HitInfo h = trace_bvh<ANY, MS>(S, ray, tmin, tmax, st, overflow, &cand);
+    HitInfo h = trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, &cand);
     if (ANY && h.prim >= 0) return h;
     if (cand.n > 0) {
       float ts;
@@ -374,12 +376,17 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
     }
     return h;
   }
-  return trace_bvh<ANY, MS>(S, ray, tmin, tmax, st, overflow, nullptr);
+  return trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, nullptr);
 }
 
 template <bool ANY, int MS>
+__device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
+                                            uint32_t &overflow, SdfCand *cand);
+
+template <bool ANY, int MS, bool SPEC>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                              uint32_t &overflow, SdfCand *cand) {
+  if (SPEC && S.use_bvh) return trace_ww<ANY, MS>(S, ray, tmin, tmax, st, overflow, cand);
   HitInfo h;
   h.t = tmax;
   h.prim = -1;
@@ -403,7 +410,8 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
     return h;
   int cur = S.root_ref;
   st.sp = 0;
-  while (true) {
+  int budget = 2 * (S.num_prims + 4) + 64;  // bounds a corrupt tree (see trace_ww)
+  while (--budget > 0) {
     if (ref_is_leaf(cur)) {
       const int first = leaf_first(cur), cnt = leaf_count(cur);
       for (int i = 0; i < cnt; ++i) {
@@ -470,6 +478,127 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
       }
     }
     if (!found) break;
+  }
+  return h;
+}
+
+// Speculative while-while traversal (Aila & Laine, "Understanding the
+// Efficiency of Ray Traversal on GPUs", HPG 2009) for the render kernels:
+// a lane that reaches a leaf postpones it and keeps visiting interior nodes
+// until every still-traversing lane of its warp holds a leaf, then the warp
+// tests its leaves together, so interior-node and primitive code run with
+// full warps instead of alternating per iteration. Leaves are tested in the
+// same front-to-back order; postponing only makes culling by the closest hit
+// less eager, so a hit can differ from the exact-order traversal only where a
+// primitive test and its box test disagree by a rounding step.
+#define RB_TRAV_DONE 0x7FFFFFFF
+
+__device__ __forceinline__ void visit_interior(const SceneView &S, const RayPre &rp, const Ray &ray, int cur, float tmin,
+                                               float closest, int &next, Stack &st, uint32_t &overflow) {
+  float tl, tr;
+  bool hl, hr;
+  int4 f3v;
+  if (!S.quantized) {
+    const float4 *n = S.nodes + 4 * (size_t)cur;
+    const float4 f0 = __ldg(n), f1 = __ldg(n + 1), f2 = __ldg(n + 2);
+    f3v = __ldg(reinterpret_cast<const int4 *>(n + 3));
+    hl = box_hit(rp, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, tmin, closest, tl);
+    hr = box_hit(rp, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, tmin, closest, tr);
+  } else {
+    const float4 *n = reinterpret_cast<const float4 *>(S.qnodes + cur);
+    const float4 q0 = __ldg(n);
+    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(n + 1));
+    const int rref = __ldg(reinterpret_cast<const int *>(n + 2));
+    const uint32_t meta = __float_as_uint(q0.w);
+    const float sx = __uint_as_float((meta & 0xFFu) << 23), sy = __uint_as_float(((meta >> 8) & 0xFFu) << 23),
+                sz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
+#define RB_DQ(word, sh, o, s) fmaf((float)(((word) >> (sh)) & 0xFFu), (s), (o))
+    hl = box_hit(rp, RB_DQ(q1.x, 0, q0.x, sx), RB_DQ(q1.x, 8, q0.y, sy), RB_DQ(q1.x, 16, q0.z, sz),
+                 RB_DQ(q1.x, 24, q0.x, sx), RB_DQ(q1.y, 0, q0.y, sy), RB_DQ(q1.y, 8, q0.z, sz), tmin, closest, tl);
+    hr = box_hit(rp, RB_DQ(q1.y, 16, q0.x, sx), RB_DQ(q1.y, 24, q0.y, sy), RB_DQ(q1.z, 0, q0.z, sz),
+                 RB_DQ(q1.z, 8, q0.x, sx), RB_DQ(q1.z, 16, q0.y, sy), RB_DQ(q1.z, 24, q0.z, sz), tmin, closest, tr);
+#undef RB_DQ
+    f3v = make_int4((int)q1.w, rref, (int)(meta >> 24), 0);
+  }
+  const float dcomp = f3v.z == 0 ? ray.d.x : (f3v.z == 1 ? ray.d.y : ray.d.z);
+  const bool left_near = dcomp >= 0.0f;
+  const int nref = left_near ? f3v.x : f3v.y, fref = left_near ? f3v.y : f3v.x;
+  const bool hn = left_near ? hl : hr, hf = left_near ? hr : hl;
+  const float tf = left_near ? tr : tl;
+  if (hn) {
+    if (hf) {
+      if (st.sp < RB_STACK) st.push(fref, tf);
+      else ++overflow;
+    }
+    next = nref;
+  } else if (hf) {
+    next = fref;
+  } else {
+    next = RB_TRAV_DONE;  // pop below
+  }
+}
+
+__device__ __forceinline__ int pop_next(Stack &st, float closest) {
+  while (st.sp > 0) {
+    const int2 e = st.pop();
+    if (__int_as_float(e.y) <= closest) return e.x;
+  }
+  return RB_TRAV_DONE;
+}
+
+template <bool ANY, int MS>
+__device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
+                                            uint32_t &overflow, SdfCand *cand) {
+  HitInfo h;
+  h.t = tmax;
+  h.prim = -1;
+  float closest = tmax;
+  const RayPre rp = prep(ray);
+  float te;
+  if (!box_hit(rp, S.root_box[0], S.root_box[1], S.root_box[2], S.root_box[3], S.root_box[4], S.root_box[5], tmin,
+               closest, te))
+    return h;
+  st.sp = 0;
+  int node = S.root_ref;
+  int leaf = RB_TRAV_DONE;  // postponed leaf
+  // every interior node and every leaf is visited at most once, so this
+  // budget is never reached by a well-formed tree; it bounds a corrupt one
+  int budget = 2 * (S.num_prims + 4) + 64;
+  while ((node != RB_TRAV_DONE || leaf != RB_TRAV_DONE) && --budget > 0) {
+    // interior phase
+    while (node != RB_TRAV_DONE && !ref_is_leaf(node) && --budget > 0) {
+      int next;
+      visit_interior(S, rp, ray, node, tmin, closest, next, st, overflow);
+      node = next == RB_TRAV_DONE ? pop_next(st, closest) : next;
+      if (node != RB_TRAV_DONE && ref_is_leaf(node) && leaf == RB_TRAV_DONE) {
+        leaf = node;  // postpone and keep descending
+        node = pop_next(st, closest);
+      }
+      if (__all_sync(__activemask(), leaf != RB_TRAV_DONE)) break;
+    }
+    // a leaf reached without a postponed one (e.g. the root is a leaf)
+    if (leaf == RB_TRAV_DONE && node != RB_TRAV_DONE && ref_is_leaf(node)) {
+      leaf = node;
+      node = pop_next(st, closest);
+    }
+    // leaf phase: the postponed leaf, then `node` if it is one too
+    while (leaf != RB_TRAV_DONE) {
+      const int first = leaf_first(leaf), cnt = leaf_count(leaf);
+      for (int i = 0; i < cnt; ++i) {
+        float t;
+        if (prim_t<MS>(S, first + i, ray, tmin, closest, t, cand)) {
+          closest = t;
+          h.t = t;
+          h.prim = first + i;
+          if (ANY) return h;
+        }
+      }
+      leaf = RB_TRAV_DONE;
+      if (node != RB_TRAV_DONE && ref_is_leaf(node)) {
+        leaf = node;
+        node = pop_next(st, closest);
+      }
+    }
   }
   return h;
 }
