@@ -286,11 +286,14 @@ bool prim_t(const Scene &S, int i, const Ray &r, double tmin, double tmax, doubl
 }
 
 // Smooth-union field of the SDF primitives whose inflated bounding spheres
-// overlap [tmin, tmax], folded in index order; sphere tracing on the field's
-// magnitude; normal by central differences (step 5e-4); material of the
-// nearest primitive.
+// overlap [tmin, tmax], folded in index order over those whose window (the
+// ray interval inside the inflated sphere) holds the current t; sphere tracing
+// on the field's magnitude, each step clamped to the next window entry;
+// normal by central differences (step 5e-4) over the hit point's windows;
+// material of the nearest primitive.
 bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &tt, D3 &n, int &mat) {
-  std::vector<int> c;
+  struct Win { int idx; double t0, t1; };
+  std::vector<Win> c;
   for (int i = 0; i < (int)S.sdf.size(); ++i) {
     const SdfP &q = S.sdf[i];
     const D3 oc = r.o - q.pos;
@@ -299,44 +302,56 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
     const double disc = hb * hb - a * cc;
     if (disc < 0) continue;
     const double sq = std::sqrt(disc), t0 = (-hb - sq) / a, t1 = (-hb + sq) / a;
-    if (t1 >= tmin && t0 <= tmax && c.size() < 24) c.push_back(i);
+    if (t1 >= tmin && t0 <= tmax && c.size() < 24) c.push_back({i, t0, t1});
   }
   if (c.empty()) return false;
-  auto field = [&](const D3 &p, int *nearest) {
-    double F = 1e30, best = 1e30;
-    for (size_t k = 0; k < c.size(); ++k) {
-      const double d = sdf_eval1(S.sdf[c[k]], p);
-      if (nearest && d < best) { best = d; *nearest = c[k]; }
-      F = k == 0 ? d : smin_poly(F, d, S.sdf_k);
+  const double FAR = 1e30;
+  auto field = [&](const D3 &p, double t, double &next, int *nearest) {
+    double F = FAR, best = FAR;
+    bool first = true;
+    next = FAR;
+    for (const Win &w : c) {
+      if (w.t0 > t) { next = std::fmin(next, w.t0); continue; }
+      if (t > w.t1) continue;
+      const double d = sdf_eval1(S.sdf[w.idx], p);
+      if (nearest && d < best) { best = d; *nearest = w.idx; }
+      F = first ? d : smin_poly(F, d, S.sdf_k);
+      first = false;
     }
     return F;
   };
   const double il = 1.0 / r.d.len();
-  double t = tmin;
-  double f0 = field(r.at(t), nullptr);
+  double t = tmin, next, nx;
+  double f0 = field(r.at(t), t, next, nullptr);
   for (int k = 0; k < 8 && std::fabs(f0) < 2.0 * S.sdf_eps; ++k) {
     t += 2.0 * S.sdf_eps * il;
-    f0 = field(r.at(t), nullptr);
+    f0 = field(r.at(t), t, next, nullptr);
   }
   const double sgn = f0 < 0 ? -1.0 : 1.0;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const D3 p = r.at(t);
-    const double F = sgn * field(p, nullptr);
+    const double raw = field(p, t, next, nullptr);
+    if (raw == FAR) {
+      if (next == FAR || next > tmax) return false;
+      t = next;
+      continue;
+    }
+    const double F = sgn * raw;
     if (F < S.sdf_eps) {
       if (t > tmax) return false;
       const double e = 5e-4;
-      const D3 gr(field(p + D3(e, 0, 0), nullptr) - field(p - D3(e, 0, 0), nullptr),
-                  field(p + D3(0, e, 0), nullptr) - field(p - D3(0, e, 0), nullptr),
-                  field(p + D3(0, 0, e), nullptr) - field(p - D3(0, 0, e), nullptr));
+      const D3 gr(field(p + D3(e, 0, 0), t, nx, nullptr) - field(p - D3(e, 0, 0), t, nx, nullptr),
+                  field(p + D3(0, e, 0), t, nx, nullptr) - field(p - D3(0, e, 0), t, nx, nullptr),
+                  field(p + D3(0, 0, e), t, nx, nullptr) - field(p - D3(0, 0, e), t, nx, nullptr));
       const double gl = gr.len();
       n = gl > 0 ? gr / gl : D3(0, 1, 0);
-      int nearest = c[0];
-      field(p, &nearest);
+      int nearest = c[0].idx;
+      field(p, t, nx, &nearest);
       mat = S.sdf[nearest].mat;
       tt = t;
       return true;
     }
-    t += F * il;
+    t = std::fmin(t + F * il, next);
     if (t > tmax) return false;
   }
   return false;

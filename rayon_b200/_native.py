@@ -9,7 +9,10 @@ import ctypes as C
 import os
 from pathlib import Path
 
-_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librayon_b200.so"
+# RAYON_B200_LIB selects another build of the same library (e.g. one compiled
+# with different -D options); the default is the in-tree build.
+_LIB_PATH = Path(os.environ.get("RAYON_B200_LIB") or
+                 Path(__file__).resolve().parent / "_lib" / "librayon_b200.so")
 
 
 class NativeLibraryMissing(RuntimeError):

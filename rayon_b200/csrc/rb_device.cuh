@@ -257,12 +257,14 @@ __device__ __forceinline__ bool t_tri(const f3 &v0, const f3 &edge1, const f3 &e
 static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &r, float tmin, float tmax);
 
 // SDF primitives of a smooth-union scene (blend radius k > 0) are not hit one
-// by one: a ray collects the ones whose k-inflated bounding spheres it crosses
-// and the union field of those is sphere-traced after the traversal.
+// by one: a ray collects the ones whose k-inflated bounding spheres it crosses,
+// each with the ray interval [t0, t1] inside its sphere, and the union field
+// of those is sphere-traced after the traversal.
 #define RB_SDF_CAND 24
 struct SdfCand {
   int n;
   int idx[RB_SDF_CAND];
+  float t0[RB_SDF_CAND], t1[RB_SDF_CAND];
 };
 
 template <int MS>
@@ -288,7 +290,12 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
       if (disc >= 0.0f) {
         const float sq = sqrtf(disc);
         const float t0 = (-hb - sq) / aa, t1 = (-hb + sq) / aa;
-        if (t1 >= tmin && t0 <= tmax && cand->n < RB_SDF_CAND) cand->idx[cand->n++] = __float_as_int(__ldg(p + 1).x);
+        if (t1 >= tmin && t0 <= tmax && cand->n < RB_SDF_CAND) {
+          cand->idx[cand->n] = __float_as_int(__ldg(p + 1).x);
+          cand->t0[cand->n] = t0;
+          cand->t1[cand->n] = t1;
+          ++cand->n;
+        }
       }
       return false;
     }
@@ -355,6 +362,11 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
 // Closest (or, with ANY, first) hit including the smooth SDF field. SPEC
 // selects the speculative while-while traversal (render kernels); without it
 // the traversal visits nodes and primitives in the reference's exact order.
+// RB_SPEC_TRAVERSAL is the render kernels' choice (build with
+// -DRB_SPEC_TRAVERSAL=0 for exact-order traversal everywhere).
+#ifndef RB_SPEC_TRAVERSAL
+#define RB_SPEC_TRAVERSAL 1
+#endif
 template <bool ANY, int MS, bool SPEC = false>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {

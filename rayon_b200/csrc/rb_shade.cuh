@@ -487,21 +487,39 @@ __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
 }
 
 // Smooth-union field of the collected SDF primitives: polynomial smooth
-// minimum (sdf.hpp:410-416) folded in primitive-index order over the
-// candidates whose inflated spheres overlap [tmin, tmax]. Sphere tracing on
-// the field's magnitude (a ray that starts inside marches to the exit), at
-// most S.sdf_steps steps, hit below S.sdf_eps; outward normal by central
-// differences with a 5e-4 step; the material is that of the nearest primitive.
+// minimum (sdf.hpp:410-416) folded in primitive-index order. A primitive takes
+// part where the ray is inside its k-inflated bounding sphere (its window
+// [t0, t1]); outside, its distance is at least k, so folding it would not
+// move the union's surface. Sphere tracing on the field's magnitude (a ray
+// that starts inside marches to the exit), each step clamped to the next
+// window entry so no primitive is stepped over, at most S.sdf_steps steps,
+// hit below S.sdf_eps; outward normal by central differences with a 5e-4 step
+// over the hit point's window set; the material is that of the nearest
+// primitive.
 #define RB_SDF_NORMAL_EPS 5e-4f
-__device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCand &c, const f3 &p, int *nearest) {
-  float F = 1e30f, best = 1e30f;
+#define RB_SDF_FAR 1e30f
+// Field at p = r.at(t) over the windows holding t; `next` is the nearest
+// window entry beyond t (RB_SDF_FAR when none). RB_SDF_FAR when no window
+// holds t.
+__device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCand &c, const f3 &p, float t,
+                                                float &next, int *nearest) {
+  float F = RB_SDF_FAR, best = RB_SDF_FAR;
+  bool first = true;
+  next = RB_SDF_FAR;
   for (int i = 0; i < c.n; ++i) {
+    const float t0 = c.t0[i];
+    if (t0 > t) {
+      next = fminf(next, t0);
+      continue;
+    }
+    if (t > c.t1[i]) continue;
     const float d = sdf_eval1(S.sdf[c.idx[i]], p);
     if (nearest && d < best) {
       best = d;
       *nearest = c.idx[i];
     }
-    F = (i == 0) ? d : smin_poly(F, d, S.sdf_k);
+    F = first ? d : smin_poly(F, d, S.sdf_k);
+    first = false;
   }
   return F;
 }
@@ -511,42 +529,57 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
   // sort candidates by index (insertion sort) so the fold order is fixed
   for (int i = 1; i < c.n; ++i) {
     const int v = c.idx[i];
+    const float a0 = c.t0[i], a1 = c.t1[i];
     int j = i - 1;
     while (j >= 0 && c.idx[j] > v) {
       c.idx[j + 1] = c.idx[j];
+      c.t0[j + 1] = c.t0[j];
+      c.t1[j + 1] = c.t1[j];
       --j;
     }
     c.idx[j + 1] = v;
+    c.t0[j + 1] = a0;
+    c.t1[j + 1] = a1;
   }
   const float inv_len = 1.0f / r.d.length();
-  float t = tmin;
+  float t = tmin, next;
   // a ray that starts in the eps shell around the surface (a bounce off the
   // field) first steps out of it, so the inside/outside decision is made
   // where the field is clearly signed
-  float f0 = sdf_field_eval(S, c, r.at(t), nullptr);
+  float f0 = sdf_field_eval(S, c, r.at(t), t, next, nullptr);
   for (int k = 0; k < 8 && fabsf(f0) < 2.0f * S.sdf_eps; ++k) {
     t += 2.0f * S.sdf_eps * inv_len;
-    f0 = sdf_field_eval(S, c, r.at(t), nullptr);
+    f0 = sdf_field_eval(S, c, r.at(t), t, next, nullptr);
   }
   const float sgn = f0 < 0.0f ? -1.0f : 1.0f;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const f3 p = r.at(t);
-    const float F = sgn * sdf_field_eval(S, c, p, nullptr);
+    const float raw = sdf_field_eval(S, c, p, t, next, nullptr);
+    if (raw == RB_SDF_FAR) {  // between windows: jump to the next entry
+      if (next == RB_SDF_FAR || next > tmax) return false;
+      t = next;
+      continue;
+    }
+    const float F = sgn * raw;
     if (F < S.sdf_eps) {
       if (t > tmax) return false;
       const float e = RB_SDF_NORMAL_EPS;
-      const f3 g(sdf_field_eval(S, c, p + f3(e, 0, 0), nullptr) - sdf_field_eval(S, c, p - f3(e, 0, 0), nullptr),
-                 sdf_field_eval(S, c, p + f3(0, e, 0), nullptr) - sdf_field_eval(S, c, p - f3(0, e, 0), nullptr),
-                 sdf_field_eval(S, c, p + f3(0, 0, e), nullptr) - sdf_field_eval(S, c, p - f3(0, 0, e), nullptr));
+      float nx;
+      const f3 g(sdf_field_eval(S, c, p + f3(e, 0, 0), t, nx, nullptr) -
+                     sdf_field_eval(S, c, p - f3(e, 0, 0), t, nx, nullptr),
+                 sdf_field_eval(S, c, p + f3(0, e, 0), t, nx, nullptr) -
+                     sdf_field_eval(S, c, p - f3(0, e, 0), t, nx, nullptr),
+                 sdf_field_eval(S, c, p + f3(0, 0, e), t, nx, nullptr) -
+                     sdf_field_eval(S, c, p - f3(0, 0, e), t, nx, nullptr));
       const float gl = g.length();
       n_out = gl > 0.0f ? g / gl : f3(0.0f, 1.0f, 0.0f);
       int nearest = c.idx[0];
-      sdf_field_eval(S, c, p, &nearest);
+      sdf_field_eval(S, c, p, t, nx, &nearest);
       mat_out = S.sdf[nearest].material;
       t_out = t;
       return true;
     }
-    t += F * inv_len;
+    t = fminf(t + F * inv_len, next);
     if (t > tmax) return false;
   }
   return false;

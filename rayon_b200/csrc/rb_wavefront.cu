@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi
   Ray r;
   r.o = f3(o.x, o.y, o.z);
   r.d = f3(d.x, d.y, d.z);
-  const HitInfo h = trace<false, MS, true>(W.S, r, 0.001f, FLT_MAX, st, ovf);
+  const HitInfo h = trace<false, MS, RB_SPEC_TRAVERSAL>(W.S, r, 0.001f, FLT_MAX, st, ovf);
   q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
   if (MS >= RB_MS_SDF && h.prim == -2) q.sn[k] = make_float4(h.sdf_n.x, h.sdf_n.y, h.sdf_n.z, __int_as_float(h.sdf_mat));
   if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfParams W, WfQueue in, WfQueu
                   Ray sr;
                   sr.o = so.ray.o;
                   sr.d = wi;
-                  const HitInfo sh = trace<true, MS, true>(W.S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
+                  const HitInfo sh = trace<true, MS, RB_SPEC_TRAVERSAL>(W.S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
                   if (sh.prim == -1) {
                     const float pl = d2 / (cl * W.S.light_area);
                     const float pb = cs * (1.0f / RB_PI);
