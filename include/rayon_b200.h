@@ -266,6 +266,20 @@ int rb_render_accumulate(const rb_cuda_scene *scene, int width, int height, cons
                          int samples_to_add, int sample_base, int max_depth, float *accum,
                          float *comp, uint64_t *counters, void *stream);
 
+/* Several views of one scene in ONE persistent launch (the batched kernel):
+ * n_views camera frames (frames: HOST, n_views x 21 doubles as rb_camera_frame
+ * writes them), all width x height, each adding samples [sample_base,
+ * sample_base + samples) per pixel. accum (DEVICE): n_views blocks of
+ * 2*width*height float4, each the view's FP32 sums followed by its Kahan
+ * compensation terms (true sum = sum - compensation). View v draws the sample
+ * streams of salt v, so view 0 repeats rb_render_accumulate's streams.
+ * counters (DEVICE, may be NULL) are overwritten with [segments, paths, stack
+ * overflows]. Extends RendererCUDAProgressive's one-view-per-launch loop
+ * (renderer_cuda_progressive_host.hpp:677-685, 904) to many views per launch. */
+int rb_render_views(const rb_cuda_scene *scene, int n_views, int width, int height, const double *frames,
+                    int samples, int sample_base, int max_depth, float *accum, uint64_t *counters,
+                    void *stream);
+
 /* Wavefront engine (an alternative to the per-pixel kernel of
  * rb_render_accumulate): SoA ray/hit queues of queue_capacity paths (0 = 2^20),
  * extend and shade kernels per bounce, warp-ballot compaction of surviving

@@ -146,6 +146,7 @@ _sig("rb_render_accumulate", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int,
      vp, vp, vp, vp)
 _sig("rb_render_wavefront", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp, C.c_int,
      vp, vp)
+_sig("rb_render_views", C.c_int, vp, C.c_int, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp, vp, vp)
 
 
 def last_error() -> str:

@@ -770,4 +770,106 @@ int rb_server_get_stats(rb_server *r, rb_server_stats *out) {
   return RB_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Several views of one scene in one persistent launch
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace rb {
+namespace {
+// Per-device job table: pinned staging, device copy, and an event that marks
+// the staging buffer free again (its last upload has run).
+struct ViewsTable {
+  unsigned char *h = nullptr, *d = nullptr;
+  size_t cap = 0;
+  cudaEvent_t uploaded = nullptr;  // staging buffer free again
+  cudaEvent_t consumed = nullptr;  // device table free again (its launch has run)
+};
+std::mutex g_views_mu;
+ViewsTable g_views[64];
+}  // namespace
+}  // namespace rb
+
+extern "C" {
+
+int rb_render_views(const rb_cuda_scene *scene, int n_views, int width, int height, const double *frames, int samples,
+                    int sample_base, int max_depth, float *accum, uint64_t *counters, void *stream) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_render_views: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  if (n_views <= 0 || n_views > 4096 || width <= 0 || height <= 0 || !frames || !accum || samples < 0 ||
+      max_depth < 0 || sample_base < 0 || (long long)width * height * n_views > (1ll << 40)) {
+    set_error("rb_render_views: invalid argument");
+    return RB_ERR_INVALID_ARG;
+  }
+  if (samples == 0) return RB_OK;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) {
+    set_error("rb_render_views: device ordinal out of range");
+    return RB_ERR_INVALID_ARG;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> lock(g_views_mu);
+  ViewsTable &T = g_views[dev];
+  const size_t bytes = sizeof(BatchCtl) + sizeof(BatchJob) * (size_t)n_views;
+  if (T.uploaded) cudaEventSynchronize(T.uploaded);  // the previous upload has left the staging buffer
+  if (bytes > T.cap) {
+    if (T.d) cudaFree(T.d);
+    if (T.h) cudaFreeHost(T.h);
+    T.d = T.h = nullptr;
+    T.cap = 0;
+    if (!cuda_ok(cudaMalloc(&T.d, bytes), "rb_render_views: job table") ||
+        !cuda_ok(cudaMallocHost(&T.h, bytes), "rb_render_views: pinned job table"))
+      return RB_ERR_CUDA;
+    T.cap = bytes;
+  }
+  if (!T.uploaded && !cuda_ok(cudaEventCreateWithFlags(&T.uploaded, cudaEventDisableTiming), "rb_render_views: event"))
+    return RB_ERR_CUDA;
+  if (!T.consumed && !cuda_ok(cudaEventCreateWithFlags(&T.consumed, cudaEventDisableTiming), "rb_render_views: event"))
+    return RB_ERR_CUDA;
+  BatchCtl *ctl = reinterpret_cast<BatchCtl *>(T.h);
+  BatchJob *jobs = reinterpret_cast<BatchJob *>(T.h + sizeof(BatchCtl));
+  std::memset(T.h, 0, bytes);
+  const Globals G = current_globals();
+  const uint32_t seed = current_opts().seed;
+  const long long px = (long long)width * height;
+  for (int v = 0; v < n_views; ++v) {
+    BatchJob &B = jobs[v];
+    B.S = ds->view;
+    B.P = frame_from(frames + 21 * (size_t)v, width, height);
+    B.P.samples = samples;
+    B.P.sample_base = sample_base;
+    B.P.max_depth = max_depth;
+    B.P.seed = seed;
+    B.P.salt = (uint32_t)v;  // view 0 draws the streams of rb_render_accumulate
+    B.G = G;
+    B.acc = reinterpret_cast<float4 *>(accum) + 2 * px * v;
+    B.task_begin = px * v;
+    B.spp_total = sample_base + samples;
+  }
+  ctl->total_tasks = (unsigned long long)(px * n_views);
+  ctl->njobs = n_views;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // a previous call's launch (possibly on another stream) must be done with the device table
+  if (!cuda_ok(cudaStreamWaitEvent(st, T.consumed, 0), "rb_render_views: wait") ||
+      !cuda_ok(cudaMemcpyAsync(T.d, T.h, bytes, cudaMemcpyHostToDevice, st), "rb_render_views: upload") ||
+      !cuda_ok(cudaEventRecord(T.uploaded, st), "rb_render_views: event"))
+    return RB_ERR_CUDA;
+  const rb_render_opts o = current_opts();
+  const int minb = o.reserved[0] > 0 ? std::min(o.reserved[0], 3) : 2;
+  BatchCtl *d_ctl = reinterpret_cast<BatchCtl *>(T.d);
+  launch_batch(ds->ms, minb, G.nee != 0, st, reinterpret_cast<const BatchJob *>(T.d + sizeof(BatchCtl)), d_ctl, sms);
+  if (!cuda_ok(cudaGetLastError(), "rb_render_views: launch")) return RB_ERR_CUDA;
+  if (counters &&
+      !cuda_ok(cudaMemcpyAsync(counters, &d_ctl->segments, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st),
+               "rb_render_views: counters"))
+    return RB_ERR_CUDA;
+  return cuda_ok(cudaEventRecord(T.consumed, st), "rb_render_views: event") ? RB_OK : RB_ERR_CUDA;
+}
+
 }  // extern "C"

@@ -128,6 +128,27 @@ def render_wavefront(ds, frame, w: int, h: int, spp: int, depth: int, background
     return (img, cnt.cpu().numpy()) if counters else img
 
 
+def render_views(ds, frames, w: int, h: int, spp: int, depth: int, background: float = 1.0,
+                 dof: tuple | None = None, nee: bool = False, sample_base: int = 0, seed: int = DEFAULT_SEED,
+                 counters: bool = False):
+    """Per-view radiance sums (n_views, h, w, 3) float64 of several camera frames
+    rendered in one persistent launch (rb_render_views); view v uses salt v."""
+    torch = _torch()
+    fr = np.ascontiguousarray(np.stack([np.asarray(f, np.float64) for f in frames]))
+    n = fr.shape[0]
+    set_globals(background=background, dof=dof)
+    acc = torch.zeros((n, 2, w * h, 4), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(4, dtype=torch.int64, device="cuda")
+    with options(nee=nee, seed=seed):
+        check(lib.rb_render_views(ds.handle, n, w, h, fr.ctypes.data_as(C.POINTER(C.c_double)), spp, sample_base,
+                                  depth, C.c_void_p(acc.data_ptr()), C.c_void_p(cnt.data_ptr()), _stream_ptr()),
+              "rb_render_views")
+        torch.cuda.synchronize()
+    set_globals()
+    img = (acc[:, 0, :, :3].double() - acc[:, 1, :, :3].double()).cpu().numpy().reshape(n, h, w, 3)
+    return (img, cnt.cpu().numpy()) if counters else img
+
+
 def render_dropin(ds, frame, w: int, h: int, spp: int, depth: int, chunks: int = 5):
     """RendererCUDA::render's loop (renderer_cuda_host.hpp:35-58) through the drop-in
     entry point with a host float3 accumulation buffer. Returns (h, w, 3) float32 sums."""
