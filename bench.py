@@ -1,20 +1,30 @@
 """Benchmark of the B200 render path (one JSON line on rank 0).
 
-Workload: the Cornell box (512x512, 256 spp, max depth 16, FP32 radiance with
-Kahan-compensated accumulation, background 0). One step = one full frame:
-512*512*256 = 67.1 M primary paths. `value` = Mpaths/s with the scene and the
-accumulation buffers resident in HBM (device time, CUDA events per step on the
-launching stream, L2 flushed between steps). `e2e` = the same frames through
-the drop-in C-ABI call exactly as RayON's offline renderer makes it
-(renderer_cuda_host.hpp:23-74): scene upload from host memory, five
-renderPixelsCUDAAccumulative calls with a host float3 accumulation buffer
-(uploaded on the first call, downloaded after every call), free.
+Default workload (the one the metric is quoted on): the Cornell box (512x512,
+256 spp, max depth 16, FP32 radiance with Kahan-compensated accumulation,
+background 0). One step = one full frame: 512*512*256 = 67.1 M primary paths.
+`value` = Mpaths/s with the scene and the accumulation buffers resident in HBM
+(device time, CUDA events per step on the launching stream, L2 flushed between
+steps). `e2e` = the same frames through the drop-in C-ABI call exactly as
+RayON's offline renderer makes it (renderer_cuda_host.hpp:23-74): scene upload
+from host memory, five renderPixelsCUDAAccumulative calls with a host float3
+accumulation buffer (uploaded on the first call, downloaded after every call),
+free.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload cornell|one_weekend|icospheres|sdf_field]
+
+The other workloads: one_weekend (400x225, 32 spp, depth 10, depth of field),
+icospheres (5.24 M triangles, 1920x1080, 64 spp, depth 8) and sdf_field (256
+SDF primitives in a smooth union, 1280x720, 128 spp, depth 8, 16 orbit views
+per step in ONE launch of rb_render_views); their e2e is scene upload + render
++ accumulation readback through the public API.
 
 --impl reference times the reference's own CPU renderer (RendererCPUParallel,
 compiled from the reference sources into oracle/_ref/) on the host cores on a
-bounded sample of the same frame.
+bounded sample of the same frame (the FP64 oracle port where that renderer
+cannot render the scene), and the reference's own CUDA renderer built for
+sm_100a on the same frame.
 """
 from __future__ import annotations
 
@@ -35,7 +45,6 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOAD = dict(name="cornell", width=512, height=512, spp=256, depth=16)
 METRIC = "Mpaths/s (Cornell box 512x512, 256 spp, depth 16)"
 
 
@@ -47,9 +56,13 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while timing."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms. Started
+    before the warm-up so that sampling is running when the timed region
+    begins; mark() brackets the timed region and summary() keeps the samples
+    taken inside it (or within 0.5 s of it when the region is shorter than
+    the sampling period)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -57,6 +70,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -69,6 +83,12 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def mark(self, start: bool) -> None:
+        if start:
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -78,23 +98,35 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
         if not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
-            if len(p) >= 9:
+            if len(p) >= 10:
+                try:
+                    p[0] = datetime.datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
                 rows.append(p)
         os.unlink(self.path)
+        window = "timed region"
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
+            if not inside:
+                inside = [r for r in rows if self.t0 - 0.5 <= r[0] <= self.t1 + 0.5]
+                window = "timed region +- 0.5 s"
+            rows = inside
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        num = lambda v: v.replace(".", "").isdigit()  # noqa: E731
+        sm = [float(r[2]) for r in rows if num(r[2])]
+        mx = [float(r[3]) for r in rows if num(r[3])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        load = sorted(sm)[len(sm) // 2:] if sm else []
-        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "window": window}
 
 
 def measured_peaks():
@@ -120,58 +152,142 @@ def profiled_traffic():
     return None
 
 
-def cpu_reference_sample(spec, budget_s: float = 12.0):
-    """RendererCPUParallel (reference sources, oracle/_ref) on a bounded sample."""
-    from oracle import refbind
-    if not refbind.host_available():
-        return None
-    r = refbind.RefScene(spec)
+def _port_sample(spec, cam, budget_s: float):
+    """The FP64 oracle (this project's CPU restatement of the path, all host
+    threads) on a seeded subset of the frame's pixels at full spp, scaled to
+    about budget_s seconds. Returns (Mpaths/s, threads, description)."""
+    from oracle.oracle import Globals, OracleScene
     w, h = spec.width, spec.height
-    secs, _, threads, rays = r.render_cpu_parallel(spec.camera, w, h, 1)
-    spp = max(1, min(spec.spp, int(budget_s / max(secs, 1e-3))))
-    if spp > 1:
-        secs, _, threads, rays = r.render_cpu_parallel(spec.camera, w, h, spp)
-    paths = w * h * spp
-    return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
-            "sample": f"RendererCPUParallel on the {w}x{h} frame at {spp} spp ({paths} paths, {secs:.1f} s; "
-                      f"FP64, linear scan, depth 16, non-Lambert materials as Lambert)",
-            "seconds": secs, "paths": paths}
+    sc = spec.to_scene()
+    sc.build_bvh()
+    o = OracleScene(sc, sdf=(spec.sdf_blend, spec.sdf_steps, spec.sdf_eps))
+    fr = cam.frame(w, h)
+    g = Globals(background=spec.background, dof=spec.dof is not None,
+                aperture=spec.dof[0] if spec.dof else 0.1, focus=spec.dof[1] if spec.dof else 10.0)
+    rng = np.random.default_rng(5)
+    n = 64
+    t = 0.0
+    while True:
+        px = rng.choice(w * h, size=n, replace=False).astype(np.int32)
+        t0 = time.perf_counter()
+        o.render(fr, w, h, spec.spp, spec.depth, g, seed=1, pixels=px)
+        t = time.perf_counter() - t0
+        if t > budget_s / 4 or n >= w * h:
+            break
+        n = min(w * h, int(n * max(2.0, budget_s / 4 / max(t, 1e-3))))
+    threads = os.cpu_count() or 1
+    return n * spec.spp / t / 1e6, threads, (f"FP64 oracle port, {n} seeded pixels of the {w}x{h} frame at "
+                                             f"{spec.spp} spp ({n * spec.spp} paths, {t:.1f} s)")
+
+
+def cpu_baseline(workload: str, spec, cam, budget_s: float = 12.0):
+    """The reference's RendererCPUParallel (compiled from its sources into
+    oracle/_ref) on a bounded spp sample of the frame where it can render the
+    scene; otherwise (5.2 M triangles by linear scan, SDF primitives) the FP64
+    oracle port on a bounded pixel sample."""
+    from oracle import refbind
+    if workload in ("cornell", "one_weekend") and refbind.host_available():
+        r = refbind.RefScene(spec)
+        w, h = spec.width, spec.height
+        secs, _, threads, rays = r.render_cpu_parallel(cam, w, h, 1)
+        spp = max(1, min(spec.spp, int(budget_s / max(secs, 1e-3))))
+        if spp > 1:
+            secs, _, threads, rays = r.render_cpu_parallel(cam, w, h, spp)
+        paths = w * h * spp
+        return {"value": paths / secs / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+                "sample": f"RendererCPUParallel on the {w}x{h} frame at {spp} spp ({paths} paths, {secs:.1f} s; "
+                          f"FP64, linear scan, depth 16, non-Lambert materials as Lambert)",
+                "seconds": secs, "paths": paths}
+    v, threads, sample = _port_sample(spec, cam, budget_s)
+    return {"value": v, "unit": "Mpaths/s", "cores": threads, "kind": "port", "sample": sample}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU renderer (RendererCPUParallel
+    from oracle/_ref) on a bounded sample per step of the same workload, on all
+    host threads; for workloads it cannot render (5.2 M triangles by linear
+    scan, SDF primitives) the FP64 oracle port. Adds the reference's own CUDA
+    renderer (renderAccKernel built for sm_100a from its sources) timed on the
+    same frame where it can render the scene."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from rayon_b200 import scenes
-    spec = scenes.cornell(**{k: WORKLOAD[k] for k in ("width", "height", "spp", "depth")})
+    spec, nviews, desc = workload_spec(args.workload)
+    cam = spec.views[0] if nviews > 1 else spec.camera
     from oracle import refbind
-    if not refbind.host_available():
+    w, h = spec.width, spec.height
+    use_ref = args.workload in ("cornell", "one_weekend")
+    if use_ref and not refbind.host_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference drivers (oracle/_ref) not built"}))
         return
-    r = refbind.RefScene(spec)
-    w, h = spec.width, spec.height
-    # bounded sample per step: spp chosen so one step is ~5 s of host work
-    secs1, _, threads, _ = r.render_cpu_parallel(spec.camera, w, h, 1)
-    spp = max(1, min(spec.spp, int(5.0 / max(secs1, 1e-3))))
-    for _ in range(args.warmup):
-        r.render_cpu_parallel(spec.camera, w, h, 1)
     times = []
-    for _ in range(args.steps):
-        s, _, threads, _ = r.render_cpu_parallel(spec.camera, w, h, spp)
-        times.append(s)
-    paths = w * h * spp
-    t = sum(times) / len(times)
-    v = paths / t / 1e6
-    print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "Mpaths/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cornell {w}x{h}, {spp} spp per step (of 256), depth 16 fixed by the renderer",
-                   "parallelism": "host threads"},
-        "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
-                         "sample": f"{w}x{h} at {spp} spp per step, RendererCPUParallel"},
+    if use_ref:
+        r = refbind.RefScene(spec)
+        # bounded sample per step: spp chosen so one step is ~5 s of host work
+        secs1, _, threads, _ = r.render_cpu_parallel(cam, w, h, 1)
+        spp = max(1, min(spec.spp, int(5.0 / max(secs1, 1e-3))))
+        for _ in range(args.warmup):
+            r.render_cpu_parallel(cam, w, h, 1)
+        for _ in range(args.steps):
+            s, _, threads, _ = r.render_cpu_parallel(cam, w, h, spp)
+            times.append(s)
+        paths = w * h * spp
+        t = sum(times) / len(times)
+        v = paths / t / 1e6
+        kind, sample = "reference", f"{w}x{h} at {spp} spp per step, RendererCPUParallel"
+        wl = f"{desc}; {spp} spp per step (of {spec.spp}), depth 16 fixed by the renderer"
+    else:
+        vals = []
+        for _ in range(max(1, min(args.steps, 3))):
+            v1, threads, sample = _port_sample(spec, cam, 5.0)
+            vals.append(v1)
+        v = sum(vals) / len(vals)
+        t = None
+        kind = "port"
+        wl = f"{desc}; bounded pixel sample per step"
+    res = {
+        "impl": "reference", "metric": METRIC if args.workload == "cornell" else f"Mpaths/s ({desc})",
+        "value": v, "unit": "Mpaths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 if t else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl, "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "Mpaths/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }))
+    }
+    if use_ref:
+        try:
+            res["reference_cuda"] = reference_cuda(spec, np.ascontiguousarray(cam.frame(w, h), np.float64))
+        except Exception as e:  # noqa: BLE001
+            res["reference_cuda"] = {"unavailable": f"{type(e).__name__}: {e}"}
+    elif args.workload == "sdf_field":
+        res["reference_cuda"] = {"unavailable": "the reference's GPU path skips SDF primitives "
+                                                "(cuda_raytracer.cuh:372-373)"}
+    else:
+        res["reference_cuda"] = {"unavailable": "not timed: the reference builds this scene's BVH single-threaded "
+                                                "(about 80 s for 5.2 M triangles)"}
+    print(json.dumps(res))
+
+
+WORKLOADS = {
+    # name: (scene constructor, views per step, description); cornell is the
+    # configuration the headline metric is quoted on
+    "cornell": ("cornell", 1, "Cornell box 512x512, 256 spp, depth 16, 30 primitives, background 0"),
+    "one_weekend": ("one_weekend", 1, "One-Weekend-style 488 spheres, 400x225, 32 spp, depth 10, depth of field"),
+    "icospheres": ("icospheres", 1, "64 level-6 icospheres (5,242,880 triangles) + ground, 1920x1080, 64 spp, "
+                                    "depth 8, GGX conductors"),
+    "sdf_field": ("sdf_field", 16, "256 SDF primitives, smooth union k=0.2, 1280x720, 128 spp, depth 8, "
+                                   "16 orbit views in one launch"),
+}
+
+
+def workload_spec(name: str, small: bool = False):
+    from rayon_b200 import scenes
+    ctor, views, desc = WORKLOADS[name]
+    spec = getattr(scenes, ctor)()
+    if small:  # profiling case: 16 spp, at most two views
+        spec.spp = 16
+        views = min(views, 2)
+    return spec, views, desc
 
 
 def main():
@@ -180,19 +296,17 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rayon_b200")
+    ap.add_argument("--workload", default="cornell", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-reference-cuda", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the equal-RMSE and serving sections")
     ap.add_argument("--small", action="store_true",
-                    help="profiling case for ncu: same frame at 16 spp, no e2e/baselines")
+                    help="profiling case for ncu: same frame at 16 spp (two views at most), no e2e/baselines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.small:
-        WORKLOAD["spp"] = 16
         args.no_cpu_baseline = True
-        args.no_reference_cuda = True
         args.no_e2e = True
 
     import torch
@@ -203,35 +317,50 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from rayon_b200 import lib, render, scenes
-    spec = scenes.cornell(**{k: WORKLOAD[k] for k in ("width", "height", "spp", "depth")})
+    from rayon_b200 import lib, render
+    spec, nviews, desc = workload_spec(args.workload, args.small)
     w, h, spp, depth = spec.width, spec.height, spec.spp, spec.depth
-    paths = w * h * spp
+    cams = spec.views[:nviews] if nviews > 1 else [spec.camera]
+    paths = w * h * spp * nviews
     sc = spec.to_scene()
     sc.build_bvh()
-    fr = np.ascontiguousarray(spec.camera.frame(w, h), np.float64)
-    ds = sc.upload(layout="autotune", tune_depth=depth, probe=(fr, w, h))
+    frames = np.ascontiguousarray(np.stack([c.frame(w, h) for c in cams]), np.float64)
+    fr = frames[0]
+    layout_kind = "autotune" if spec.n < (1 << 20) else "as_built"
+
+    def upload():
+        if layout_kind == "autotune":
+            return sc.upload(layout="autotune", tune_depth=depth, probe=(fr, w, h))
+        return sc.upload()
+
+    ds = upload()
     layout = ds.layout
-    frp = fr.ctypes.data_as(C.POINTER(C.c_double))
-    render.set_globals(background=spec.background)
+    frp = frames.ctypes.data_as(C.POINTER(C.c_double))
+    render.set_globals(background=spec.background, dof=spec.dof)
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
-    acc = torch.zeros((w * h, 4), dtype=torch.float32, device="cuda")
-    comp = torch.zeros_like(acc)
+    npx = w * h
+    acc = torch.zeros((nviews, 2, npx, 4), dtype=torch.float32, device="cuda")  # sums, Kahan terms per view
     counters = torch.zeros(4, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
 
     def step(i, cnt=None):
-        st = lib.rb_render_accumulate(ds.handle, w, h, frp, spp, (rank * 1000003 + i) * spp % (1 << 30), depth,
-                                      C.c_void_p(acc.data_ptr()), C.c_void_p(comp.data_ptr()),
-                                      C.c_void_p(cnt.data_ptr()) if cnt is not None else None, sptr)
+        base = (rank * 1000003 + i) * spp % (1 << 30)
+        cp = C.c_void_p(cnt.data_ptr()) if cnt is not None else None
+        if nviews > 1:
+            st = lib.rb_render_views(ds.handle, nviews, w, h, frp, spp, base, depth, C.c_void_p(acc.data_ptr()),
+                                     cp, sptr)
+        else:
+            st = lib.rb_render_accumulate(ds.handle, w, h, frp, spp, base, depth, C.c_void_p(acc.data_ptr()),
+                                          C.c_void_p(acc.data_ptr() + npx * 16), cp, sptr)
         if st != 0:
             raise RuntimeError(render.lib.rb_last_error().decode())
 
+    clk = ClockSampler(local).__enter__()
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
-    # segment / path counts of one frame (for Mrays/s and the work-based roofline)
+    # segment / path counts of one step (for Mrays/s)
     counters.zero_()
     step(0, counters)
     torch.cuda.synchronize()
@@ -245,15 +374,17 @@ def main():
     # NVTX range "timed" lets a profiler select the timed launches only
     # (ncu --nvtx --nvtx-include "timed/"), past the layout probes and warm-up
     torch.cuda.nvtx.range_push("timed")
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.fill_(float(i))
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            step(args.warmup + i)
-            b.record(stream)
-            evs.append((a, b))
-        torch.cuda.synchronize()
+    clk.mark(True)
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step(args.warmup + i)
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    clk.mark(False)
+    clk.__exit__(None, None, None)
     torch.cuda.nvtx.range_pop()
     launches = lib.rb_launch_count() - launches0
     ms = [a.elapsed_time(b) for a, b in evs]
@@ -265,46 +396,70 @@ def main():
         torch.distributed.barrier()
     value = world * paths / (t_ms * 1e-3) / 1e6
 
-    # ---- e2e: the drop-in call with host buffers, as the reference's offline renderer
+    # ---- e2e through the public API with host buffers
     e2e = None
-    h2d = d2h = 0
     mean_rad = None
     if not getattr(args, "no_e2e", False):
         torch.cuda.synchronize()
         e2e_times = []
-        for i in range(max(1, min(3, args.steps))):
+        reps = max(1, min(3 if paths < (1 << 28) else 1, args.steps))
+        parts = []
+        for i in range(reps):
             t0 = time.perf_counter()
-            ds2 = sc.upload(layout="autotune", tune_depth=depth, probe=(fr, w, h))  # decision cached per scene
-            img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
+            ds2 = upload()  # layout decision cached per scene
+            t_up = time.perf_counter()
+            if args.workload == "cornell":
+                # the drop-in call sequence of RayON's offline renderer
+                img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
+                h2d = ds2.nbytes + npx * 12
+                d2h = 5 * npx * 12
+            elif nviews > 1:
+                img = render.render_views(ds2, list(frames), w, h, spp, depth, background=spec.background,
+                                          dof=spec.dof)
+                h2d = ds2.nbytes + frames.nbytes
+                d2h = nviews * npx * 32
+            else:
+                img = render.render_accumulate(ds2, fr, w, h, spp, depth, background=spec.background,
+                                               dof=spec.dof)
+                h2d = ds2.nbytes
+                d2h = npx * 32
+            t_r = time.perf_counter()
             ds2.free()
             torch.cuda.synchronize()
-            e2e_times.append(time.perf_counter() - t0)
-            h2d = ds.nbytes + w * h * 12
-            d2h = 5 * w * h * 12
+            t_end = time.perf_counter()
+            e2e_times.append(t_end - t0)
+            parts.append({"upload_s": t_up - t0, "render_and_readback_s": t_r - t_up, "free_s": t_end - t_r})
+        render.set_globals(background=spec.background, dof=spec.dof)
         e2e_t = min(e2e_times)
+        breakdown = parts[e2e_times.index(e2e_t)]
         if world > 1:  # the slowest rank bounds the job
             tt = torch.tensor([e2e_t], device="cuda")
             torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
             e2e_t = float(tt.item())
+        path = ("renderPixelsCUDAAccumulative x5 + scene upload (host float3 accumulation)"
+                if args.workload == "cornell" else
+                ("scene upload + rb_render_views + accumulation readback" if nviews > 1 else
+                 "scene upload + rb_render_accumulate + accumulation readback"))
         e2e = {"value": world * paths / e2e_t / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_t,
-               "path": "renderPixelsCUDAAccumulative x5 + scene upload (host float3 accumulation)"}
-        mean_rad = float(img.reshape(-1, 3).mean() / spp)
+               "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_t, "path": path,
+               "breakdown": breakdown, "all_seconds": e2e_times}
+        mean_rad = float(np.asarray(img).reshape(-1, 3).mean() / spp)
 
     peaks, peaks_kind = measured_peaks()
     # roofline of the render kernel: its DRAM-bound bytes are the accumulation
     # state (sum + Kahan compensation, read and written: 64 B per pixel); the
-    # scene (~2 KB) lives in L1. The kernel is bound by instruction issue, so
-    # the issue roof is reported beside it from counted work.
-    alg_bytes = w * h * 64
+    # scene of the small workloads lives in L1/L2. The kernel is bound by
+    # instruction issue, reported beside it.
+    alg_bytes = npx * nviews * 64
     achieved = alg_bytes / (t_ms * 1e-3) / 1e9
-    sm_mhz = None
     res = {
-        "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "metric": f"Mpaths/s ({desc})" if args.workload != "cornell" else METRIC,
+        "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"cornell {w}x{h}, {spp} spp, depth {depth}, 30 primitives, background 0",
-                   "paths_per_step": paths, "kernel": "k_render (per-pixel, flattened sample x bounce loop)",
+        "config": {"workload": desc, "paths_per_step": paths,
+                   "kernel": ("k_batch (persistent, one launch for all views)" if nviews > 1 else
+                              "k_render (per-pixel, flattened sample x bounce loop)"),
                    "layout": layout,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "mrays_per_s": world * segs / (t_ms * 1e-3) / 1e6,
@@ -316,21 +471,19 @@ def main():
     clocks = clk.summary()
     res["clocks"] = clocks
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    traffic = profiled_traffic() if args.workload == "cornell" else None
     res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                       "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(),
+                       "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                        "peak_kind": f"{peaks_kind} HBM copy bandwidth",
                        "algorithmic_bytes_per_launch": alg_bytes}
-    if rank == 0 and world == 1 and not args.no_reference_cuda:
-        res["reference_cuda"] = reference_cuda(spec, fr)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            res["cpu_baseline"] = cpu_reference_sample(spec)
+            res["cpu_baseline"] = cpu_baseline(args.workload, spec, cams[0])
         except Exception as e:  # noqa: BLE001
             res["cpu_baseline"] = {"unavailable": str(e)}
-    res["fp32_issue_peak_tflops_at_clock"] = fp32_peak
+    res["fp32_issue_peak_tflops_at_clock"] = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     res["mean_radiance"] = mean_rad
-    if rank == 0 and world == 1 and not args.small and not args.no_extras:
+    if rank == 0 and world == 1 and args.workload == "cornell" and not args.small and not args.no_extras:
         for key, fn in (("equal_rmse", lambda: equal_rmse_section(t_ms, paths)),
                         ("serving", lambda: serving_section())):
             try:
@@ -362,6 +515,8 @@ def reference_cuda(spec, fr):
     secs = L.refc_render(sh, w, h, frp, spec.spp, 5, spec.depth, None)
     L.refc_scene_destroy(sh)
     best = min(ms)
+    if best <= 0:
+        return {"unavailable": "the reference's CUDA render call failed (see its printed error)"}
     paths = w * h * spec.spp
     return {"mpaths_s": paths / (best * 1e-3) / 1e6, "ms_per_frame": best,
             "e2e_mpaths_s": paths / secs / 1e6 if secs > 0 else None,
@@ -427,23 +582,23 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
 
 
 def equal_rmse_section(full_ms_plain: float, full_paths: int):
-    """Estimator efficiency at equal RMSE against the FP64 oracle (Cornell box
-    at 64x64): RMSE of 64-spp renders with and without next-event estimation
-    against an FP64 oracle image at 4096 spp (NEE), combined with each
-    estimator's Mpaths/s on the full 512x512 frame."""
+    """Estimator efficiency at equal RMSE (Cornell box at 64x64): RMSE of
+    64-spp renders with and without next-event estimation against the FP64
+    oracle's converged image (4096 spp, NEE; the committed fixture
+    tests/golden/oracle_cornell64.npz made by tests/golden/make_golden.py
+    --oracle), combined with each estimator's Mpaths/s on the full 512x512
+    frame."""
     import torch
 
-    from oracle.oracle import Globals, OracleScene
     from rayon_b200 import lib, render, scenes
     spec = scenes.cornell(width=64, height=64)
     sc = spec.to_scene()
     sc.build_bvh()
     ds = sc.upload(layout="autotune", tune_depth=spec.depth)
     fr = spec.camera.frame(64, 64)
-    t0 = time.time()
-    ref, _ = OracleScene(sc).render(fr, 64, 64, 4096, spec.depth, Globals(background=0.0, nee=True), seed=777)
-    oracle_s = time.time() - t0
-    ref = ref.reshape(64, 64, 3) / 4096
+    fx = np.load(ROOT / "tests" / "golden" / "oracle_cornell64.npz")
+    ref = fx["mean"].astype(np.float64)
+    oracle_s = float(fx["seconds"])
     out = {}
     for nee in (False, True):
         errs = []

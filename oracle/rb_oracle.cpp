@@ -104,7 +104,6 @@ struct Scene {
   double sdf_k = 0;
   int sdf_steps = 256;
   double sdf_eps = 1e-4;
-  double sdf_omega = 1.5;  // over-relaxation of the field march (the GPU's RB_SDF_OMEGA)
 };
 
 struct Counters {
@@ -329,26 +328,15 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
     f0 = field(r.at(t), t, next, nullptr);
   }
   const double sgn = f0 < 0 ? -1.0 : 1.0;
-  // over-relaxed steps (Keinert et al. 2014) with the return to a plain step
-  // when consecutive unbounding spheres do not overlap or the field changed sign
-  const double len = r.d.len();
-  double omega = S.sdf_omega, t_prev = -1.0, F_prev = 0.0, next_prev = FAR;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const D3 p = r.at(t);
     const double raw = field(p, t, next, nullptr);
     if (raw == FAR) {
       if (next == FAR || next > tmax) return false;
       t = next;
-      t_prev = -1.0;
       continue;
     }
     const double F = sgn * raw;
-    if (omega > 1.0 && t_prev >= 0.0 && (F < 0.0 || F + F_prev < (t - t_prev) * len)) {
-      omega = 1.0;
-      t = std::fmin(t_prev + F_prev * il, next_prev);
-      t_prev = -1.0;
-      continue;
-    }
     if (F < S.sdf_eps) {
       if (t > tmax) return false;
       const double e = 5e-4;
@@ -363,10 +351,7 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
       tt = t;
       return true;
     }
-    t_prev = t;
-    F_prev = F;
-    next_prev = next;
-    t = std::fmin(t + omega * F * il, next);
+    t = std::fmin(t + F * il, next);
     if (t > tmax) return false;
   }
   return false;

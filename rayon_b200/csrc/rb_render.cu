@@ -547,10 +547,19 @@ __global__ void k_f3_to_f4(const float *__restrict__ in, float4 *__restrict__ ou
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.0f);
 }
-__global__ void k_f4_to_f3(const float4 *__restrict__ in, float *__restrict__ out, int n) {
+// float4 sums (minus their Kahan compensation terms when comp is given) to
+// the host's float3 layout
+__global__ void k_f4_to_f3(const float4 *__restrict__ in, const float4 *__restrict__ comp, float *__restrict__ out,
+                           int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
-    const float4 v = in[i];
+    float4 v = in[i];
+    if (comp) {
+      const float4 c = comp[i];
+      v.x -= c.x;
+      v.y -= c.y;
+      v.z -= c.z;
+    }
     out[3 * i] = v.x;
     out[3 * i + 1] = v.y;
     out[3 * i + 2] = v.z;
@@ -592,6 +601,10 @@ static int default_minb(int ms, bool nee) {
   return nee ? 1 : 2;
 }
 static void default_block(int ms, int &bx, int &by) {
+  if (ms == RB_MS_SDF) {  // 8x8 tiles keep a warp's marching rays together
+    bx = by = 8;
+    return;
+  }
   bx = ms >= RB_MS_FULL ? 32 : 16;
   by = ms >= RB_MS_FULL ? 4 : 8;
 }
@@ -918,6 +931,43 @@ void resetDeviceAccumBuffer(void *p, int num_pixels) {
   cuda_ok(cudaMemset(p, 0, bytes), "resetDeviceAccumBuffer");
 }
 
+}  // extern "C"
+
+namespace rb {
+namespace {
+// float3 staging of the drop-in's host accumulation buffer, kept per device
+// across calls (the reference converts through a host loop; here a kernel
+// converts on the device and one pinned copy crosses PCIe): a device float3
+// array and a pinned host mirror, grown on demand, freed at exit.
+struct F3Stage {
+  float *dev = nullptr, *host = nullptr;
+  size_t bytes = 0;
+};
+F3Stage g_f3_stage[64];
+std::mutex g_stage_mu;
+
+F3Stage *f3_stage(size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  F3Stage &S = g_f3_stage[dev];
+  if (S.bytes < bytes) {
+    if (S.dev) cudaFree(S.dev);
+    if (S.host) cudaFreeHost(S.host);
+    S.dev = S.host = nullptr;
+    S.bytes = 0;
+    if (!cuda_ok(cudaMalloc(&S.dev, bytes), "cudaMalloc(accum staging)") ||
+        !cuda_ok(cudaMallocHost(&S.host, bytes), "cudaMallocHost(accum staging)"))
+      return nullptr;
+    S.bytes = bytes;
+  }
+  return &S;
+}
+}  // namespace
+}  // namespace rb
+
+extern "C" {
+
 unsigned long long renderPixelsCUDAAccumulative(
     unsigned char *image, float *accum_buffer, rb_cuda_scene *scene, int width, int height, double ccx,
     double ccy, double ccz, double p0x, double p0y, double p0z, double dux, double duy, double duz, double dvx,
@@ -958,13 +1008,14 @@ unsigned long long renderPixelsCUDAAccumulative(
     }
     cudaMemsetAsync(acc, 0, 2 * nb, st);
     if (accum_buffer) {
-      float *tmp = nullptr;
-      if (!cuda_ok(cudaMalloc(&tmp, (size_t)n * 12), "cudaMalloc(accum staging)")) return 0ull;
-      cudaMemcpyAsync(tmp, accum_buffer, (size_t)n * 12, cudaMemcpyHostToDevice, st);
-      k_f3_to_f4<<<(n + 255) / 256, 256, 0, st>>>(tmp, acc, n);
+      std::lock_guard<std::mutex> lk(g_stage_mu);
+      F3Stage *S = f3_stage((size_t)n * 12);
+      if (!S) return 0ull;
+      std::memcpy(S->host, accum_buffer, (size_t)n * 12);
+      cudaMemcpyAsync(S->dev, S->host, (size_t)n * 12, cudaMemcpyHostToDevice, st);
+      k_f3_to_f4<<<(n + 255) / 256, 256, 0, st>>>(S->dev, acc, n);
       g_launches++;
-      cudaStreamSynchronize(st);
-      cudaFree(tmp);
+      if (!cuda_ok(cudaStreamSynchronize(st), "accum upload")) return 0ull;
     }
   } else {
     acc = static_cast<float4 *>(*d_accum_buffer_ptr);
@@ -999,12 +1050,13 @@ unsigned long long renderPixelsCUDAAccumulative(
                   nullptr, st);
   cuda_ok(cudaStreamSynchronize(st), "renderPixelsCUDAAccumulative");
   if (accum_buffer) {
-    float *tmp = nullptr;
-    if (cuda_ok(cudaMalloc(&tmp, (size_t)n * 12), "cudaMalloc(accum staging)")) {
-      k_f4_to_f3<<<(n + 255) / 256, 256, 0, st>>>(acc, tmp, n);
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    F3Stage *S = f3_stage((size_t)n * 12);
+    if (S) {
+      k_f4_to_f3<<<(n + 255) / 256, 256, 0, st>>>(acc, comp, S->dev, n);
       g_launches++;
-      cuda_ok(cudaMemcpy(accum_buffer, tmp, (size_t)n * 12, cudaMemcpyDeviceToHost), "accum download");
-      cudaFree(tmp);
+      cudaMemcpyAsync(S->host, S->dev, (size_t)n * 12, cudaMemcpyDeviceToHost, st);
+      if (cuda_ok(cudaStreamSynchronize(st), "accum download")) std::memcpy(accum_buffer, S->host, (size_t)n * 12);
     }
   }
   return (unsigned long long)n * (unsigned long long)samples_to_add;

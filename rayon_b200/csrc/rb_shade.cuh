@@ -498,9 +498,6 @@ __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
 // primitive.
 #define RB_SDF_NORMAL_EPS 5e-4f
 #define RB_SDF_FAR 1e30f
-#ifndef RB_SDF_OMEGA
-#define RB_SDF_OMEGA 1.5f
-#endif
 // Field at p = r.at(t) over the windows holding t; `next` is the nearest
 // window entry beyond t (RB_SDF_FAR when none). RB_SDF_FAR when no window
 // holds t.
@@ -555,29 +552,15 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
     f0 = sdf_field_eval(S, c, r.at(t), t, next, nullptr);
   }
   const float sgn = f0 < 0.0f ? -1.0f : 1.0f;
-  // over-relaxed sphere tracing (Keinert et al., "Enhanced Sphere Tracing",
-  // 2014): steps of RB_SDF_OMEGA x F; when the unbounding spheres of the
-  // previous and the new point do not overlap, the relaxed step may have
-  // crossed the surface (as it has when the field changed sign), so the march
-  // returns to the previous point, takes the plain step and stays plain
-  const float len = r.d.length();
-  float omega = RB_SDF_OMEGA, t_prev = -1.0f, F_prev = 0.0f, next_prev = RB_SDF_FAR;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const f3 p = r.at(t);
     const float raw = sdf_field_eval(S, c, p, t, next, nullptr);
     if (raw == RB_SDF_FAR) {  // between windows: jump to the next entry
       if (next == RB_SDF_FAR || next > tmax) return false;
       t = next;
-      t_prev = -1.0f;
       continue;
     }
     const float F = sgn * raw;
-    if (omega > 1.0f && t_prev >= 0.0f && (F < 0.0f || F + F_prev < (t - t_prev) * len)) {
-      omega = 1.0f;
-      t = fminf(t_prev + F_prev * inv_len, next_prev);
-      t_prev = -1.0f;
-      continue;
-    }
     if (F < S.sdf_eps) {
       if (t > tmax) return false;
       const float e = RB_SDF_NORMAL_EPS;
@@ -596,10 +579,7 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
       t_out = t;
       return true;
     }
-    t_prev = t;
-    F_prev = F;
-    next_prev = next;
-    t = fminf(t + omega * F * inv_len, next);
+    t = fminf(t + F * inv_len, next);
     if (t > tmax) return false;
   }
   return false;

@@ -2,6 +2,7 @@
 
   python tests/golden/make_golden.py --bvh        (CPU; needs oracle/_ref/librayon_ref_host.so)
   python tests/golden/make_golden.py --gpu OUTDIR (GPU; needs oracle/_ref/librayon_ref_cuda.so)
+  python tests/golden/make_golden.py --oracle     (CPU; needs oracle/_build/liboracle.so)
 
 --bvh: for each BVH case, the scene is built through the reference's
 SceneDescription (addSphere / addRectangle / addTriangle) and its buildBVH;
@@ -9,6 +10,9 @@ the node array and the leaf-order permutation are saved (bvh_<case>.npz).
 --gpu: for each hit case, pixel-centre primary-hit ids and distances from the
 reference's own hit_aabb / intersect_geometry on the GPU (hits_<case>.npz),
 and reference CUDA renders of small scenes (refimg_<case>.npz) for RMSE checks.
+--oracle: the FP64 oracle's converged Cornell box at 64x64 (4096 spp, next-event
+estimation, background 0, seed 777), the ground truth of the benchmark's
+equal-RMSE comparison (oracle_cornell64.npz).
 """
 from __future__ import annotations
 
@@ -99,11 +103,31 @@ def make_gpu(out: Path) -> None:
         L.refc_scene_destroy(sh)
 
 
+def make_oracle(out: Path) -> None:
+    import time
+
+    from oracle.oracle import Globals, OracleScene
+    from rayon_b200 import scenes
+    spec = scenes.cornell(width=64, height=64)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    fr = spec.camera.frame(64, 64)
+    t0 = time.time()
+    ref, _ = OracleScene(sc).render(fr, 64, 64, 4096, spec.depth, Globals(background=0.0, nee=True), seed=777)
+    secs = time.time() - t0
+    img = (ref.reshape(64, 64, 3) / 4096).astype(np.float32)
+    np.savez_compressed(out / "oracle_cornell64.npz", mean=img, spp=4096, depth=spec.depth, seed=777, seconds=secs)
+    print("oracle_cornell64 mean", img.reshape(-1, 3).mean(0), "secs", secs)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--bvh", action="store_true")
     ap.add_argument("--gpu", default=None)
+    ap.add_argument("--oracle", action="store_true")
     a = ap.parse_args()
+    if a.oracle:
+        make_oracle(HERE)
     if a.bvh:
         make_bvh(HERE)
     if a.gpu:
