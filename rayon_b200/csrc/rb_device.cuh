@@ -121,15 +121,20 @@ struct LightRec {      // one emitter sampled by next-event estimation
   float pad;
 };
 
-struct SdfPrim {       // one SDF primitive (ray marched)
+// One SDF primitive (ray marched): 5 x 16 B, read by the field march as five
+// 128-bit loads. Position, parameters a b c, rounding radius (ROUND_BOX),
+// type, world->local rotation r00..r22, material.
+struct __align__(16) SdfPrim {
+  float px, py, pz, a;
+  float b, c, round;
   int type;
+  float r00, r01, r02, r10;
+  float r11, r12, r20, r21;
+  float r22;
   int material;
-  float px, py, pz;    // position
-  float a, b, c;       // parameters
-  float round;         // rounding radius (ROUND_BOX)
-  float r00, r01, r02, r10, r11, r12, r20, r21, r22;  // world->local rotation
   float pad[2];
 };
+static_assert(sizeof(SdfPrim) == 80, "SdfPrim is five 16-byte words");
 
 // Kernel-parameter view of a device scene (passed by value).
 struct SceneView {

@@ -481,6 +481,19 @@ __device__ __forceinline__ float sdf_eval1(const SdfPrim &q, const f3 &pw) {
   }
 }
 
+// sdf_eval1 of primitive i of the table, its record read as five 128-bit loads.
+__device__ __forceinline__ float sdf_eval_at(const SdfPrim *__restrict__ tab, int i, const f3 &pw) {
+  const float4 *v = reinterpret_cast<const float4 *>(tab + i);
+  const float4 w0 = __ldg(v), w1 = __ldg(v + 1), w2 = __ldg(v + 2), w3 = __ldg(v + 3), w4 = __ldg(v + 4);
+  SdfPrim q;
+  q.px = w0.x; q.py = w0.y; q.pz = w0.z; q.a = w0.w;
+  q.b = w1.x; q.c = w1.y; q.round = w1.z; q.type = __float_as_int(w1.w);
+  q.r00 = w2.x; q.r01 = w2.y; q.r02 = w2.z; q.r10 = w2.w;
+  q.r11 = w3.x; q.r12 = w3.y; q.r20 = w3.z; q.r21 = w3.w;
+  q.r22 = w4.x;
+  return sdf_eval1(q, pw);
+}
+
 __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
   const float h = fminf(fmaxf(0.5f + 0.5f * (d2 - d1) / k, 0.0f), 1.0f);
   return d2 * (1.0f - h) + d1 * h - k * h * (1.0f - h);
@@ -513,7 +526,7 @@ __device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCan
       continue;
     }
     if (t > c.t1[i]) continue;
-    const float d = sdf_eval1(S.sdf[c.idx[i]], p);
+    const float d = sdf_eval_at(S.sdf, c.idx[i], p);
     if (nearest && d < best) {
       best = d;
       *nearest = c.idx[i];
@@ -524,9 +537,8 @@ __device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCan
   return F;
 }
 
-static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax,
-                                                    SdfCand &c, float &t_out, f3 &n_out, int &mat_out) {
-  // sort candidates by index (insertion sort) so the fold order is fixed
+// Candidates sorted by primitive index (insertion sort) so the fold order is fixed.
+__device__ __forceinline__ void sdf_sort_cand(SdfCand &c) {
   for (int i = 1; i < c.n; ++i) {
     const int v = c.idx[i];
     const float a0 = c.t0[i], a1 = c.t1[i];
@@ -541,6 +553,11 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
     c.t0[j + 1] = a0;
     c.t1[j + 1] = a1;
   }
+}
+
+static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax,
+                                                    SdfCand &c, float &t_out, f3 &n_out, int &mat_out) {
+  sdf_sort_cand(c);
   const float inv_len = 1.0f / r.d.length();
   float t = tmin, next;
   // a ray that starts in the eps shell around the surface (a bounce off the

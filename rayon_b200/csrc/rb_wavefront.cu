@@ -16,6 +16,13 @@
 //           are written compacted into queue B: each warp ballots its lanes
 //           that produce a path, one lane reserves the warp's range with one
 //           atomic, lanes write at their rank.
+// Scenes with a smooth SDF field add a third launch between the two: extend
+// only collects each ray's field candidates (sorted by primitive index, one
+// 16-byte record per candidate: index and window [t0, t1]) and appends the
+// ray to a march list; march is a persistent kernel whose lanes each take a
+// ray from the list, advance it one sphere-tracing step per pass and take
+// the next ray as soon as theirs finishes, so a warp does not wait for its
+// slowest ray (a march takes from one to hundreds of steps).
 // The queues then swap. Work items are sample-major (consecutive lanes take
 // consecutive pixels of the same sample) so primary rays of a warp are
 // coherent and the accumulation atomics of a warp hit distinct pixels. The
@@ -48,6 +55,9 @@ struct WfCtl {
   unsigned long long segments;
   unsigned long long paths_done;
   unsigned long long overflow;
+  int march_count;                // rays appended to the march list this iteration
+  unsigned int march_next;        // next march-list entry to take
+  unsigned long long march_steps;
 };
 
 struct WfParams {
@@ -56,7 +66,17 @@ struct WfParams {
   FrameF P;      // P.samples = samples per pixel of the launch, P.sample_base first sample
   double *acc;   // w*h*4 doubles (xyz sums, pad)
   WfCtl *ctl;
+  // smooth SDF field (null otherwise): candidate records of queue slot k at
+  // cand[i * cap + k], i < ncand[k]; list = slots to march
+  int4 *cand;
+  int *ncand;
+  int *list;
+  int cap;
 };
+
+__device__ __forceinline__ bool wf_marches(const WfParams &W) {
+  return W.cand != nullptr && W.S.sdf_k > 0.0f && W.S.num_sdf > 0;
+}
 
 // Generates the camera ray of work item `item` into queue slot `k`.
 __device__ __forceinline__ void wf_emit_camera(const WfParams &W, const WfQueue &q, int k, unsigned long long item) {
@@ -88,23 +108,225 @@ template <int MS>
 __global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi) {
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= W.ctl->count[qi]) return;
-  Stack st;
-  st.sh = smem + threadIdx.x;
-  st.stride = blockDim.x;
-  uint32_t ovf = 0;
-  const float4 o = q.o[k], d = q.d[k];
-  Ray r;
-  r.o = f3(o.x, o.y, o.z);
-  r.d = f3(d.x, d.y, d.z);
-  const HitInfo h = trace<false, MS, RB_SPEC_TRAVERSAL>(W.S, r, 0.001f, FLT_MAX, st, ovf);
-  q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
-  if (MS >= RB_MS_SDF && h.prim == -2) q.sn[k] = make_float4(h.sdf_n.x, h.sdf_n.y, h.sdf_n.z, __int_as_float(h.sdf_mat));
-  if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
+  const int lane = threadIdx.x & 31;
+  const bool valid = k < W.ctl->count[qi];
+  bool march = false;
+  if (valid) {
+    Stack st;
+    st.sh = smem + threadIdx.x;
+    st.stride = blockDim.x;
+    uint32_t ovf = 0;
+    const float4 o = q.o[k], d = q.d[k];
+    Ray r;
+    r.o = f3(o.x, o.y, o.z);
+    r.d = f3(d.x, d.y, d.z);
+    if (MS >= RB_MS_SDF && wf_marches(W)) {
+      // traversal only: the field is marched by k_wf_march
+      SdfCand cand;
+      cand.n = 0;
+      const HitInfo h = trace_bvh<false, MS, RB_SPEC_TRAVERSAL>(W.S, r, 0.001f, FLT_MAX, st, ovf, &cand);
+      q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
+      if (cand.n > 0) {
+        sdf_sort_cand(cand);
+        for (int i = 0; i < cand.n; ++i)
+          W.cand[(size_t)i * W.cap + k] =
+              make_int4(cand.idx[i], __float_as_int(cand.t0[i]), __float_as_int(cand.t1[i]), 0);
+        W.ncand[k] = cand.n;
+        march = true;
+      }
+    } else {
+      const HitInfo h = trace<false, MS, RB_SPEC_TRAVERSAL>(W.S, r, 0.001f, FLT_MAX, st, ovf);
+      q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
+      if (MS >= RB_MS_SDF && h.prim == -2)
+        q.sn[k] = make_float4(h.sdf_n.x, h.sdf_n.y, h.sdf_n.z, __int_as_float(h.sdf_mat));
+    }
+    if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
+  }
+  if (MS >= RB_MS_SDF) {
+    // append the warp's marching rays to the list (one atomic per warp)
+    const unsigned mask = __ballot_sync(0xffffffffu, march);
+    if (mask) {
+      int base = 0;
+      const int leader = __ffs(mask) - 1;
+      if (lane == leader) base = atomicAdd(&W.ctl->march_count, __popc(mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (march) W.list[base + __popc(mask & ((1u << lane) - 1u))] = k;
+    }
+  }
 }
 
+// Field of the candidates of queue slot `slot` (the same operations, in the
+// same order, as sdf_field_eval over an in-register candidate list). The first
+// WF_CAND_REG candidate records are passed in registers (loaded once per ray),
+// the rest are read from the slot's records.
+#define WF_CAND_REG 4
+struct WfFold {
+  float F = RB_SDF_FAR, best = RB_SDF_FAR, next = RB_SDF_FAR;
+  bool first = true;
+  __device__ __forceinline__ void add(const SceneView &S, const int4 e, const f3 &p, float t, int *nearest) {
+    const float t0 = __int_as_float(e.y);
+    if (t0 > t) {
+      next = fminf(next, t0);
+      return;
+    }
+    if (t > __int_as_float(e.z)) return;
+    const float d = sdf_eval_at(S.sdf, e.x, p);
+    if (nearest && d < best) {
+      best = d;
+      *nearest = e.x;
+    }
+    F = first ? d : smin_poly(F, d, S.sdf_k);
+    first = false;
+  }
+};
+
+__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, int slot, int n,
+                                          const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
+                                          int *nearest) {
+  WfFold f;
+#pragma unroll
+  for (int i = 0; i < WF_CAND_REG; ++i)
+    if (i < n) f.add(S, cr[i], p, t, nearest);
+  for (int i = WF_CAND_REG; i < n; ++i) f.add(S, __ldg(W.cand + (size_t)i * W.cap + slot), p, t, nearest);
+  next = f.next;
+  return f.F;
+}
+
+// Persistent field march over the march list. Every pass, each busy lane
+// evaluates the field exactly once, whatever its phase, so the warp's lanes
+// evaluate in lockstep: escape (stepping out of the eps shell, up to 8
+// passes), march (one sphere-tracing step of sdf_field_march's loop) and, at
+// a hit, the six central differences of the normal (one per pass). The
+// nearest primitive (the hit's material) is tracked in every march
+// evaluation, which at the hit is the evaluation at the hit point itself. A
+// lane whose ray finishes (hit, windows left behind, closest primitive hit
+// passed, steps used up) takes the next ray from the list (one atomic per
+// warp). A field hit replaces the ray's hit record.
+enum : int { WF_ESCAPE = 0, WF_MARCH = 1, WF_NORMAL = 2 };
+
+template <int MS>
+__global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q) {
+  const int lane = threadIdx.x & 31;
+  const SceneView &S = W.S;
+  const unsigned total = (unsigned)W.ctl->march_count;
+  const float e = RB_SDF_NORMAL_EPS;
+  int slot = 0, n = 0, steps = 0, phase = WF_ESCAPE, sub = 0, nearest = 0;
+  int4 cr[WF_CAND_REG];
+#pragma unroll
+  for (int i = 0; i < WF_CAND_REG; ++i) cr[i] = make_int4(0, 0, 0, 0);
+  float t = 0.f, tmax = 0.f, sgn = 1.f, inv_len = 1.f;
+  f3 p(0.f, 0.f, 0.f), g(0.f, 0.f, 0.f);
+  Ray r;
+  r.o = r.d = f3(0.f, 0.f, 0.f);
+  bool busy = false, drained = false;
+  unsigned long long passes = 0;
+  while (true) {
+    const bool need = !busy && !drained;
+    const unsigned mask = __ballot_sync(0xffffffffu, need);
+    if (mask) {
+      unsigned base = 0;
+      const int leader = __ffs(mask) - 1;
+      if (lane == leader) base = atomicAdd(&W.ctl->march_next, (unsigned)__popc(mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
+        if (idx < total) {
+          slot = W.list[idx];
+          n = W.ncand[slot];
+#pragma unroll
+          for (int i = 0; i < WF_CAND_REG; ++i)
+            if (i < n) cr[i] = __ldg(W.cand + (size_t)i * W.cap + slot);
+          const float4 o = q.o[slot], d = q.d[slot];
+          r.o = f3(o.x, o.y, o.z);
+          r.d = f3(d.x, d.y, d.z);
+          tmax = q.hit[slot].x;
+          inv_len = 1.0f / r.d.length();
+          t = 0.001f;
+          phase = WF_ESCAPE;
+          sub = 0;
+          steps = 0;
+          busy = true;
+        } else {
+          drained = true;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, busy) == 0) break;
+    if (!busy) continue;
+    ++passes;
+    // the one evaluation of this pass
+    f3 pe;
+    if (phase == WF_NORMAL) {
+      const float off = (sub & 1) ? -e : e;
+      pe = p + f3(sub < 2 ? off : 0.f, (sub >> 1) == 1 ? off : 0.f, sub >= 4 ? off : 0.f);
+    } else {
+      pe = r.at(t);
+    }
+    float next;
+    int near = cr[0].x;
+    const float raw = wf_field(S, W, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near);
+    bool finished = false;
+    if (phase == WF_NORMAL) {
+      if (sub & 1) {
+        if (sub == 1) g.x = g.x - raw;
+        else if (sub == 3) g.y = g.y - raw;
+        else g.z = g.z - raw;
+      } else {
+        if (sub == 0) g.x = raw;
+        else if (sub == 2) g.y = raw;
+        else g.z = raw;
+      }
+      if (++sub == 6) {
+        const float gl = g.length();
+        const f3 nv = gl > 0.0f ? g / gl : f3(0.0f, 1.0f, 0.0f);
+        q.hit[slot] = make_float4(t, __int_as_float(-2), 0.f, 0.f);
+        q.sn[slot] = make_float4(nv.x, nv.y, nv.z, __int_as_float(S.sdf[nearest].material));
+        finished = true;
+      }
+    } else {
+      if (phase == WF_ESCAPE) {
+        if (fabsf(raw) < 2.0f * S.sdf_eps && sub < 8) {
+          t += 2.0f * S.sdf_eps * inv_len;
+          ++sub;
+        } else {
+          sgn = raw < 0.0f ? -1.0f : 1.0f;
+          phase = WF_MARCH;  // and this evaluation is the first march step's
+        }
+      }
+      if (phase == WF_MARCH) {
+        if (raw == RB_SDF_FAR) {  // between windows: jump to the next entry
+          if (next == RB_SDF_FAR || next > tmax) finished = true;
+          else t = next;
+        } else {
+          const float F = sgn * raw;
+          if (F < S.sdf_eps) {
+            if (t <= tmax) {
+              p = pe;
+              nearest = near;
+              phase = WF_NORMAL;
+              sub = 0;
+            } else {
+              finished = true;
+            }
+          } else {
+            t = fminf(t + F * inv_len, next);
+            if (t > tmax) finished = true;
+          }
+        }
+        if (!finished && phase == WF_MARCH && ++steps >= S.sdf_steps) finished = true;
+      }
+    }
+    if (finished) busy = false;
+  }
+  for (int o2 = 16; o2 > 0; o2 >>= 1) passes += __shfl_down_sync(0xffffffffu, passes, o2);
+  if (lane == 0 && passes) atomicAdd(&W.ctl->march_steps, passes);
+}
+
+#ifndef WF_SHADE_MINB
+#define WF_SHADE_MINB 2
+#endif
 template <int MS, bool NEE>
-__global__ void __launch_bounds__(256) k_wf_shade(WfParams W, WfQueue in, WfQueue out, int qi) {
+__global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQueue in, WfQueue out, int qi) {
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -259,8 +481,12 @@ __global__ void __launch_bounds__(256) k_wf_shade(WfParams W, WfQueue in, WfQueu
   if (lane == 0 && s) atomicAdd(&W.ctl->segments, s);
 }
 
-// Resets the live count of the queue the next shade writes into.
-__global__ void k_wf_reset(WfCtl *ctl, int qi) { ctl->count[qi] = 0; }
+// Resets the live count of the queue the next shade writes into, and the march list.
+__global__ void k_wf_reset(WfCtl *ctl, int qi) {
+  ctl->count[qi] = 0;
+  ctl->march_count = 0;
+  ctl->march_next = 0;
+}
 
 struct WfEngine {
   int capacity = 0;
@@ -268,6 +494,11 @@ struct WfEngine {
   WfCtl *ctl = nullptr;
   WfCtl *h_ctl = nullptr;
   cudaStream_t st = nullptr;
+  // smooth-SDF march buffers, allocated on first use: RB_SDF_CAND x capacity
+  // candidate records, counts and the march list
+  int4 *cand = nullptr;
+  int *ncand = nullptr;
+  int *list = nullptr;
 };
 
 static void wf_free(WfEngine &E) {
@@ -277,6 +508,18 @@ static void wf_free(WfEngine &E) {
   }
   cudaFree(E.ctl);
   cudaFreeHost(E.h_ctl);
+  cudaFree(E.cand);
+  cudaFree(E.ncand);
+  cudaFree(E.list);
+  E.cand = nullptr;
+  E.ncand = E.list = nullptr;
+}
+
+static bool wf_alloc_march(WfEngine &E) {
+  if (E.cand) return true;
+  return cuda_ok(cudaMalloc(&E.cand, sizeof(int4) * RB_SDF_CAND * (size_t)E.capacity), "wavefront candidates") &&
+         cuda_ok(cudaMalloc(&E.ncand, sizeof(int) * (size_t)E.capacity), "wavefront candidates") &&
+         cuda_ok(cudaMalloc(&E.list, sizeof(int) * (size_t)E.capacity), "wavefront march list");
 }
 
 static bool wf_alloc(WfEngine &E, int capacity) {
@@ -298,23 +541,32 @@ static bool wf_alloc(WfEngine &E, int capacity) {
 }
 
 template <int MS, bool NEE>
-static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, cudaStream_t st) {
+static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int march_grid, cudaStream_t st) {
   const size_t sm = sizeof(int2) * RB_SHORT * 256;
   k_wf_reset<<<1, 1, 0, st>>>(E.ctl, qi ^ 1);
   k_wf_extend<MS><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
+  if (march_grid > 0) k_wf_march<MS><<<march_grid, 256, 0, st>>>(W, E.q[qi]);
   k_wf_shade<MS, NEE><<<grid, 256, sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
 }
 
 template <int MS, bool NEE>
 static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   const int grid = (E.capacity + 255) / 256;
+  int march_grid = 0;
+  if (MS >= RB_MS_SDF && W.cand) {  // persistent march: the resident blocks
+    int per_sm = 0, dev = 0, sms = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS>, 256, 0);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    march_grid = std::max(1, per_sm) * sms;
+  }
   k_wf_fill<<<grid, 256, 0, st>>>(W, E.q[0], 0, E.capacity);
   g_launches++;
   // eight iterations per graph (queues 0->1->0 ...), replayed until empty
   cudaGraph_t g = nullptr;
   cudaGraphExec_t ge = nullptr;
   if (!cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "wavefront capture")) return RB_ERR_CUDA;
-  for (int i = 0; i < 8; ++i) wf_iteration<MS, NEE>(W, E, i & 1, grid, st);
+  for (int i = 0; i < 8; ++i) wf_iteration<MS, NEE>(W, E, i & 1, grid, march_grid, st);
   const cudaError_t ec = cudaStreamEndCapture(st, &g);  // always end the capture, also after an error
   if (!cuda_ok(ec, "wavefront capture") || !g) return RB_ERR_CUDA;
   const bool inst = cuda_ok(cudaGraphInstantiate(&ge, g, 0), "wavefront graph");
@@ -323,7 +575,7 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   int it = 0;
   for (int guard = 0; guard < 1 << 20; ++guard) {
     cudaGraphLaunch(ge, st);
-    g_launches += 24;
+    g_launches += march_grid > 0 ? 32 : 24;
     it += 8;
     cudaMemcpyAsync(E.h_ctl, E.ctl, sizeof(WfCtl), cudaMemcpyDeviceToHost, st);
     if (!cuda_ok(cudaStreamSynchronize(st), "wavefront iteration")) {
@@ -365,10 +617,6 @@ extern "C" int rb_render_wavefront(const rb_cuda_scene *scene, int width, int he
   if (!priv[dev] && !cuda_ok(cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking), "wavefront stream"))
     return RB_ERR_CUDA;
   cudaStream_t st = priv[dev];
-  cudaEvent_t fence;
-  cudaEventCreateWithFlags(&fence, cudaEventDisableTiming);
-  cudaEventRecord(fence, caller);
-  cudaStreamWaitEvent(st, fence, 0);
   // queues are kept per (device, capacity) between calls: a render loop pays
   // for their allocation once (2 x 7 arrays of capacity x 16 B)
   const int cap = queue_capacity > 0 ? queue_capacity : (1 << 20);
@@ -395,6 +643,17 @@ extern "C" int rb_render_wavefront(const rb_cuda_scene *scene, int width, int he
   W.P.salt = 0;
   W.acc = accum;
   W.ctl = E.ctl;
+  if (ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0) {
+    if (!wf_alloc_march(E)) return RB_ERR_OUT_OF_MEMORY;
+    W.cand = E.cand;
+    W.ncand = E.ncand;
+    W.list = E.list;
+    W.cap = E.capacity;
+  }
+  cudaEvent_t fence;
+  if (!cuda_ok(cudaEventCreateWithFlags(&fence, cudaEventDisableTiming), "wavefront fence")) return RB_ERR_CUDA;
+  cudaEventRecord(fence, caller);
+  cudaStreamWaitEvent(st, fence, 0);
   WfCtl init;
   std::memset(&init, 0, sizeof init);
   init.total_paths = (unsigned long long)width * height * samples;

@@ -70,3 +70,24 @@ def test_sdf_field_primary_hits_match_oracle(cuda):
     assert field.mean() > 0.03, "the SDF field should cover part of the image"
     assert (field == (oids == -2)).mean() > 0.97
     ds.free()
+
+
+@pytest.mark.parametrize("nee", [False, True])
+def test_sdf_field_wavefront_paired_with_per_pixel_kernel(cuda, nee):
+    # the wavefront engine marches the field in its own persistent kernel
+    # (rays taken from a march list) with the per-pixel kernel's arithmetic:
+    # the same sample streams give the same paths
+    spec = scenes.sdf_field(count=48, width=64, height=36, spp=8, depth=4)
+    w, h, spp = 64, 36, 8
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = spec.camera.frame(w, h)
+    a = render.render_accumulate(ds, fr, w, h, spp, spec.depth, background=spec.background, nee=nee)
+    b, cnt = render.render_wavefront(ds, fr, w, h, spp, spec.depth, background=spec.background, nee=nee,
+                                     queue_capacity=4096, counters=True)
+    assert int(cnt[1]) == w * h * spp
+    bad = (np.abs(a - b) > 2e-3 * (1 + np.abs(a)) * spp).any(axis=2)
+    assert bad.mean() < MAX_DIVERGED, bad.mean()
+    np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=2e-2, atol=1e-3)
+    ds.free()
