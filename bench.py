@@ -276,8 +276,11 @@ WORKLOADS = {
     "icospheres": ("icospheres", 1, "64 level-6 icospheres (5,242,880 triangles) + ground, 1920x1080, 64 spp, "
                                     "depth 8, GGX conductors"),
     "sdf_field": ("sdf_field", 16, "256 SDF primitives, smooth union k=0.2, 1280x720, 128 spp, depth 8, "
-                                   "16 orbit views in one launch"),
+                                   "16 orbit views in one wavefront run"),
 }
+# engine per workload: the per-pixel / batched kernel, or the wavefront engine
+# (whose separate field-march kernel is the faster one for SDF fields)
+ENGINE = {"sdf_field": "wavefront"}
 
 
 def workload_spec(name: str, small: bool = False):
@@ -340,14 +343,21 @@ def main():
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
     npx = w * h
-    acc = torch.zeros((nviews, 2, npx, 4), dtype=torch.float32, device="cuda")  # sums, Kahan terms per view
+    engine = ENGINE.get(args.workload, "kernel")
+    if engine == "wavefront":  # FP64 sums per view
+        acc = torch.zeros((nviews, npx, 4), dtype=torch.float64, device="cuda")
+    else:  # FP32 sums and Kahan terms per view
+        acc = torch.zeros((nviews, 2, npx, 4), dtype=torch.float32, device="cuda")
     counters = torch.zeros(4, dtype=torch.int64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > 126 MB L2
 
     def step(i, cnt=None):
         base = (rank * 1000003 + i) * spp % (1 << 30)
         cp = C.c_void_p(cnt.data_ptr()) if cnt is not None else None
-        if nviews > 1:
+        if engine == "wavefront":
+            st = lib.rb_render_views_wavefront(ds.handle, nviews, w, h, frp, spp, base, depth,
+                                               C.c_void_p(acc.data_ptr()), 1 << 22, cp, sptr)
+        elif nviews > 1:
             st = lib.rb_render_views(ds.handle, nviews, w, h, frp, spp, base, depth, C.c_void_p(acc.data_ptr()),
                                      cp, sptr)
         else:
@@ -413,6 +423,11 @@ def main():
                 img = render.render_dropin(ds2, fr, w, h, spp, depth, chunks=5)
                 h2d = ds2.nbytes + npx * 12
                 d2h = 5 * npx * 12
+            elif engine == "wavefront":
+                img = render.render_views_wavefront(ds2, list(frames), w, h, spp, depth, background=spec.background,
+                                                    dof=spec.dof, queue_capacity=1 << 22)
+                h2d = ds2.nbytes + frames.nbytes
+                d2h = nviews * npx * 32
             elif nviews > 1:
                 img = render.render_views(ds2, list(frames), w, h, spp, depth, background=spec.background,
                                           dof=spec.dof)
@@ -438,7 +453,8 @@ def main():
             e2e_t = float(tt.item())
         path = ("renderPixelsCUDAAccumulative x5 + scene upload (host float3 accumulation)"
                 if args.workload == "cornell" else
-                ("scene upload + rb_render_views + accumulation readback" if nviews > 1 else
+                ("scene upload + rb_render_views_wavefront + accumulation readback" if engine == "wavefront" else
+                 "scene upload + rb_render_views + accumulation readback" if nviews > 1 else
                  "scene upload + rb_render_accumulate + accumulation readback"))
         e2e = {"value": world * paths / e2e_t / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_t, "path": path,
@@ -458,7 +474,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": desc, "paths_per_step": paths,
-                   "kernel": ("k_batch (persistent, one launch for all views)" if nviews > 1 else
+                   "kernel": ("wavefront engine (k_wf_extend / k_wf_march / k_wf_shade over shared SoA queues "
+                              "for all views)" if engine == "wavefront" else
+                              "k_batch (persistent, one launch for all views)" if nviews > 1 else
                               "k_render (per-pixel, flattened sample x bounce loop)"),
                    "layout": layout,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},

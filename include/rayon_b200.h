@@ -293,6 +293,16 @@ int rb_render_wavefront(const rb_cuda_scene *scene, int width, int height, const
                         int queue_capacity, uint64_t *counters, void *stream);
 
 /* Number of kernel launches this library has made (all entry points). */
+/* rb_render_views on the wavefront engine: the rays of all n_views views run
+ * in one persistent wavefront (shared SoA queues, one job table, paths
+ * regenerated across views), with FP64 accumulation. accum (DEVICE): n_views
+ * blocks of width*height*4 doubles (xyz sums, pad), added to. Same sample
+ * streams as rb_render_views (view v on salt v). counters (DEVICE, may be
+ * NULL): [segments, paths, stack overflows, iterations]. */
+int rb_render_views_wavefront(const rb_cuda_scene *scene, int n_views, int width, int height,
+                              const double *frames, int samples, int sample_base, int max_depth,
+                              double *accum, int queue_capacity, uint64_t *counters, void *stream);
+
 unsigned long long rb_launch_count(void);
 
 /* ======================================================================== */
@@ -327,7 +337,9 @@ typedef struct rb_server_opts {
   int use_graph;                /* 1: each iteration is a CUDA graph launch */
   int frames_every;             /* > 0: write each active job's u8 frame every N iterations */
   int occupancy;                /* resident 256-thread blocks per SM (0 = tuned) */
-  int reserved[3];
+  int wavefront_field;          /* 1 (default): jobs of scenes with a smooth SDF field run on the
+                                   wavefront engine (FP64 accumulation); 0: batched kernel */
+  int reserved[2];
 } rb_server_opts;
 
 void rb_server_default_opts(rb_server_opts *out);

@@ -147,6 +147,8 @@ _sig("rb_render_accumulate", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int,
 _sig("rb_render_wavefront", C.c_int, vp, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp, C.c_int,
      vp, vp)
 _sig("rb_render_views", C.c_int, vp, C.c_int, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp, vp, vp)
+_sig("rb_render_views_wavefront", C.c_int, vp, C.c_int, C.c_int, C.c_int, c_double_p, C.c_int, C.c_int, C.c_int, vp,
+     C.c_int, vp, vp)
 
 
 def last_error() -> str:
@@ -171,7 +173,7 @@ class JobRequest(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_int64), ("max_active_jobs", C.c_int), ("paths_per_iteration", C.c_int64),
                 ("max_spp_per_iteration", C.c_int), ("use_graph", C.c_int), ("frames_every", C.c_int),
-                ("occupancy", C.c_int), ("reserved", C.c_int * 3)]
+                ("occupancy", C.c_int), ("wavefront_field", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class JobStatus(C.Structure):

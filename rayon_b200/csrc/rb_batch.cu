@@ -298,12 +298,21 @@ static int64_t job_bytes(const rb_job_request &r, bool frames) {
   return (f64 ? n * 32 : n * 32) + (frames ? n * 4 : 0);
 }
 
+// Jobs of scenes with a smooth SDF field run on the wavefront engine, whose
+// field march keeps a warp's lanes stepping together (see rb_wavefront.cu).
+#define RB_WF_GROUP RB_GROUPS
+static bool on_wavefront(const Server &S, const Job &J) {
+  if (!S.o.wavefront_field) return false;
+  const rbd::SceneView &v = S.scenes[J.req.scene]->view;
+  return S.scenes[J.req.scene]->ms >= RB_MS_SDF && v.sdf_k > 0.0f && v.num_sdf > 0;
+}
+
 static bool admit(Server &S, Job &J) {
   const bool frames = S.o.frames_every > 0;
   const int64_t need = job_bytes(J.req, frames);
   if (S.used_bytes + need > S.o.memory_budget_bytes || (int)S.active.size() >= S.o.max_active_jobs) return false;
   const int64_t n = (int64_t)J.req.width * J.req.height;
-  const bool f64 = J.req.fp64_accum || J.req.spp > 65536;
+  const bool f64 = J.req.fp64_accum || J.req.spp > 65536 || on_wavefront(S, J);
   cudaError_t e;
   if (f64) {
     e = cudaMallocAsync((void **)&J.acc64, n * 32, S.st);
@@ -370,7 +379,8 @@ static int server_step(Server &S) {
     const double rem = (double)J.req.width * J.req.height * (J.req.spp - J.spp_done);
     const double age = tnow - J.t_arrival;
     // group key: kernel class, plus 4 when the job uses next-event estimation
-    cand.push_back({id, 0, S.scenes[J.req.scene]->ms + (J.req.nee ? 4 : 0), rem / (1.0 + S.aging * age)});
+    const int cls = on_wavefront(S, J) ? RB_WF_GROUP : S.scenes[J.req.scene]->ms + (J.req.nee ? 4 : 0);
+    cand.push_back({id, 0, cls, rem / (1.0 + S.aging * age)});
   }
   std::stable_sort(cand.begin(), cand.end(), [](const Plan &a, const Plan &b) { return a.prio < b.prio; });
   int64_t budget = S.o.paths_per_iteration;
@@ -395,16 +405,21 @@ static int server_step(Server &S) {
   long long tb = 0;
   std::memset(S.h_ctl, 0, sizeof(BatchCtl) * RB_GROUPS);
   int jfirst[RB_GROUPS] = {0};
+  std::vector<size_t> wf_k;  // planned jobs that run on the wavefront engine (sorted last)
   for (size_t k = 0; k < plan.size(); ++k) {
     Job &J = S.jobs[plan[k].id];
     const DeviceScene *ds = S.scenes[J.req.scene];
     const int cls = plan[k].cls;
-    BatchCtl &C = S.h_ctl[cls];
-    if (C.njobs == 0) {
-      jfirst[cls] = (int)k;
-      C.next_task = (unsigned long long)tb;
+    if (cls == RB_WF_GROUP) {
+      wf_k.push_back(k);
+    } else {
+      BatchCtl &C = S.h_ctl[cls];
+      if (C.njobs == 0) {
+        jfirst[cls] = (int)k;
+        C.next_task = (unsigned long long)tb;
+      }
+      C.njobs++;
     }
-    C.njobs++;
     BatchJob &B = S.h_jobs[k];
     std::memset(&B, 0, sizeof B);
     B.S = ds->view;
@@ -430,7 +445,7 @@ static int server_step(Server &S) {
                                                      B.spp_total >= J.req.spp);
     B.frame = frame_now ? J.frame : nullptr;
     tb += (long long)J.req.width * J.req.height;
-    C.total_tasks = (unsigned long long)tb;
+    if (cls != RB_WF_GROUP) S.h_ctl[cls].total_tasks = (unsigned long long)tb;
   }
   for (int c = 1; c < RB_GROUPS; ++c) S.h_ctl[c].job_offset = jfirst[c];
   S.h_ctl[0].total_tasks = (unsigned long long)tb;             // all jobs (frames)
@@ -448,8 +463,36 @@ static int server_step(Server &S) {
     for (int c = 1; c < RB_GROUPS; ++c)
       if (all_groups || S.h_ctl[c].njobs > 0) launch_group(c);
   };
+  // wavefront jobs: one engine run per scene over its planned jobs
+  uint64_t wf_paths = 0, wf_segments = 0;
+  auto run_wavefront = [&]() -> int {
+    std::vector<int> scenes;
+    for (size_t k : wf_k) {
+      const int sc = S.jobs[plan[k].id].req.scene;
+      if (std::find(scenes.begin(), scenes.end(), sc) == scenes.end()) scenes.push_back(sc);
+    }
+    for (int sc : scenes) {
+      std::vector<WfJob> wj;
+      for (size_t k : wf_k) {
+        const Job &J = S.jobs[plan[k].id];
+        if (J.req.scene != sc) continue;
+        WfJob w;
+        std::memset(&w, 0, sizeof w);
+        w.P = S.h_jobs[k].P;
+        w.G = S.h_jobs[k].G;
+        w.acc = J.acc64;
+        wj.push_back(w);
+      }
+      uint64_t c[4] = {0, 0, 0, 0};
+      const int rc = wf_render_jobs(S.scenes[sc], wj.data(), (int)wj.size(), 1 << 22, c, S.st);
+      if (rc != RB_OK) return rc;
+      wf_segments += c[0];
+      wf_paths += c[1];
+    }
+    return RB_OK;
+  };
   const long long frame_blocks_cap = (S.o.paths_per_iteration + 255) / 256 + 1;
-  if (S.o.use_graph && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
+  if (S.o.use_graph && wf_k.empty() && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
     // One graph, reused every iteration: table and control blocks are copied
     // from pinned staging when the graph runs, the three class kernels are
     // persistent (grid = resident blocks) and exit at once when their class
@@ -476,6 +519,10 @@ static int server_step(Server &S) {
     cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
     cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
     kernels(false);
+    if (!wf_k.empty()) {
+      const int rc = run_wavefront();
+      if (rc != RB_OK) return rc;
+    }
     if (frames) {
       k_batch_frames<<<(unsigned)((tb + 255) / 256), 256, 0, S.st>>>(S.d_jobs, S.d_ctl);
       g_launches++;
@@ -492,6 +539,8 @@ static int server_step(Server &S) {
     S.stats.paths += (int64_t)S.h_ctl[c].paths;
     S.stats.segments += (int64_t)S.h_ctl[c].segments;
   }
+  S.stats.paths += (int64_t)wf_paths;
+  S.stats.segments += (int64_t)wf_segments;
   if (frames) S.stats.frames += (int64_t)plan.size();
   // retire
   const double t = S.now();
@@ -548,6 +597,7 @@ void rb_server_default_opts(rb_server_opts *o) {
   o->max_spp_per_iteration = 64;
   o->use_graph = 1;
   o->frames_every = 0;
+  o->wavefront_field = 1;
 }
 
 rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {

@@ -58,6 +58,25 @@ struct FrameF {
   float adaptive_threshold;
 };
 
+// One job of a wavefront-engine run: its camera frame (P.samples samples per
+// pixel from P.sample_base, P.max_depth, stream seed and salt), shading
+// settings, FP64 accumulation (w*h*4 doubles: xyz sums, pad) and its first
+// work item (set by wf_render_jobs). Work items are job-major, then
+// sample-major within the job.
+struct __align__(16) WfJob {
+  FrameF P;
+  rbd::Globals G;
+  double *acc;
+  unsigned long long item_begin;
+};
+
+struct DeviceScene;
+// Renders the jobs (host table) of one scene on the wavefront engine until
+// every path has ended, ordered after and before `caller`. counters (host,
+// may be null): segments, paths, stack overflows, iterations.
+int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capacity, uint64_t *counters,
+                   cudaStream_t caller);
+
 bool cuda_ok(cudaError_t e, const char *what);
 void set_error(const std::string &msg);
 DeviceScene *lookup_scene(const void *handle);

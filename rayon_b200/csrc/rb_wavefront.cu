@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <vector>
 
 #include "rb_path.cuh"
 
@@ -62,9 +63,8 @@ struct WfCtl {
 
 struct WfParams {
   SceneView S;
-  Globals G;
-  FrameF P;      // P.samples = samples per pixel of the launch, P.sample_base first sample
-  double *acc;   // w*h*4 doubles (xyz sums, pad)
+  const WfJob *jobs;  // device table of njobs jobs
+  int njobs;
   WfCtl *ctl;
   // smooth SDF field (null otherwise): candidate records of queue slot k at
   // cand[i * cap + k], i < ncand[k]; list = slots to march
@@ -78,18 +78,32 @@ __device__ __forceinline__ bool wf_marches(const WfParams &W) {
   return W.cand != nullptr && W.S.sdf_k > 0.0f && W.S.num_sdf > 0;
 }
 
-// Generates the camera ray of work item `item` into queue slot `k`.
+__device__ __forceinline__ int wf_find_job(const WfParams &W, unsigned long long item) {
+  int lo = 0, hi = W.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&W.jobs[mid].item_begin) <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Generates the camera ray of work item `item` into queue slot `k`; the
+// path's meta record carries (pixel, job, bounce, path key).
 __device__ __forceinline__ void wf_emit_camera(const WfParams &W, const WfQueue &q, int k, unsigned long long item) {
-  const int npix = W.P.width * W.P.height;
-  const int pix = (int)(item % (unsigned long long)npix);
-  const int sample = (int)(item / (unsigned long long)npix);
-  const uint32_t key = rb_path_key(W.P.seed, W.P.salt, (uint32_t)pix, (uint32_t)(W.P.sample_base + sample));
-  const Ray r = camera_ray(W.P, W.G, pix % W.P.width, pix / W.P.width, key);
+  const int j = wf_find_job(W, item);
+  const WfJob &J = W.jobs[j];
+  const unsigned long long local = item - J.item_begin;
+  const int npix = J.P.width * J.P.height;
+  const int pix = (int)(local % (unsigned long long)npix);
+  const int sample = (int)(local / (unsigned long long)npix);
+  const uint32_t key = rb_path_key(J.P.seed, J.P.salt, (uint32_t)pix, (uint32_t)(J.P.sample_base + sample));
+  const Ray r = camera_ray(J.P, J.G, pix % J.P.width, pix / J.P.width, key);
   q.o[k] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
   q.d[k] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
   q.thr[k] = make_float4(1.f, 1.f, 1.f, 0.f);
   q.L[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-  q.meta[k] = make_int4(pix, sample, 0, (int)key);
+  q.meta[k] = make_int4(pix, j, 0, (int)key);
 }
 
 // Initial fill of queue `qi` with min(capacity, total) fresh paths.
@@ -343,6 +357,8 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
     uint32_t ovf = 0;
     const float4 o = in.o[k], d = in.d[k], th = in.thr[k], Lv = in.L[k], hv = in.hit[k];
     const int4 m = in.meta[k];
+    const Globals G = W.jobs[m.y].G;
+    const int max_depth = W.jobs[m.y].P.max_depth;
     Ray ray;
     ray.o = f3(o.x, o.y, o.z);
     ray.d = f3(d.x, d.y, d.z);
@@ -361,21 +377,21 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
     // shade with the precomputed hit (path_segment's body after its trace)
     bool ended = false;
     if (h.prim == -1) {
-      if (W.G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * W.G.background_intensity;
+      if (G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * G.background_intensity;
       ended = true;
     } else {
       const Surface sf = surface<MS>(W.S, ray, h);
       if (!sf.visible && bounce == 0) {
         ray.o = sf.p + ray.d * 0.01f;
-        ended = ++bounce >= W.P.max_depth;
+        ended = ++bounce >= max_depth;
       } else if (sf.mat >= W.S.num_mats) {
         ended = true;
       } else {
         const DevMaterial &mt = W.S.mats[sf.mat];
-        const ScatterOut so = scatter<MS>(W.G, mt, sf, ray, key, bounce);
+        const ScatterOut so = scatter<MS>(G, mt, sf, ray, key, bounce);
         if (so.emit.length_squared() > 0.0f) {
           float wgt = 1.0f;
-          if (NEE && W.G.nee && prev_pdf > 0.0f && mt.kind == L_LIGHT && W.S.num_lights > 0) {
+          if (NEE && G.nee && prev_pdf > 0.0f && mt.kind == L_LIGHT && W.S.num_lights > 0) {
             const float dl = h.t * ray.d.length();
             const float cl = fabsf(dot(sf.n, normalize(ray.d)));
             const float pl = cl > 0.0f ? dl * dl / (cl * W.S.light_area) : 0.0f;
@@ -386,12 +402,12 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
         if (!so.scattered) {
           ended = true;
         } else {
-          if (NEE && W.G.nee) {
+          if (NEE && G.nee) {
             prev_pdf = 0.0f;
-            if (mt.kind == L_LAMBERTIAN && bounce + 1 < W.P.max_depth && W.S.num_lights > 0) {
+            if (mt.kind == L_LAMBERTIAN && bounce + 1 < max_depth && W.S.num_lights > 0) {
               LightSample ls;
               const uint32_t dl = rb_vdim(bounce, RB_SLOT_LIGHT);
-              if (sample_light(W.S, W.G, rb_draw(key, dl), rb_draw(key, dl + 1), rb_draw(key, dl + 2), ls)) {
+              if (sample_light(W.S, G, rb_draw(key, dl), rb_draw(key, dl + 1), rb_draw(key, dl + 2), ls)) {
                 const f3 dv = ls.p - so.ray.o;
                 const float d2 = dv.length_squared();
                 const float dist = sqrtf(d2);
@@ -421,13 +437,13 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
           }
           if (!ended) {
             ray = so.ray;
-            ended = ++bounce >= W.P.max_depth;
+            ended = ++bounce >= max_depth;
           }
         }
       }
     }
     if (ended) {
-      double *a = W.acc + 4 * (size_t)m.x;
+      double *a = W.jobs[m.y].acc + 4 * (size_t)m.x;
       atomicAdd(a, (double)L.x);
       atomicAdd(a + 1, (double)L.y);
       atomicAdd(a + 2, (double)L.z);
@@ -499,6 +515,10 @@ struct WfEngine {
   int4 *cand = nullptr;
   int *ncand = nullptr;
   int *list = nullptr;
+  // job table: pinned staging and device copy
+  WfJob *h_jobs = nullptr;
+  WfJob *d_jobs = nullptr;
+  int jobs_cap = 0;
 };
 
 static void wf_free(WfEngine &E) {
@@ -513,6 +533,10 @@ static void wf_free(WfEngine &E) {
   cudaFree(E.list);
   E.cand = nullptr;
   E.ncand = E.list = nullptr;
+  cudaFreeHost(E.h_jobs);
+  cudaFree(E.d_jobs);
+  E.h_jobs = E.d_jobs = nullptr;
+  E.jobs_cap = 0;
 }
 
 static bool wf_alloc_march(WfEngine &E) {
@@ -589,6 +613,112 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   return RB_OK;
 }
 
+
+// Runs the engine over `njobs` jobs of one scene (host job table; item_begin
+// filled here) until every path has ended. The engine records its iterations
+// into a CUDA graph, which needs a capturable stream: it runs on a private
+// non-blocking stream ordered after the caller's stream on entry and before
+// it on return. Queues, march buffers and the job table are kept per
+// (thread, device) between calls. counters (host, may be null): segments,
+// paths, stack overflows, iterations.
+int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capacity, uint64_t *counters,
+                   cudaStream_t caller) {
+  static thread_local cudaStream_t priv[64] = {nullptr};
+  static thread_local WfEngine cached[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return RB_ERR_UNSUPPORTED;
+  if (!priv[dev] && !cuda_ok(cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking), "wavefront stream"))
+    return RB_ERR_CUDA;
+  cudaStream_t st = priv[dev];
+  const int cap = queue_capacity > 0 ? queue_capacity : (1 << 20);
+  WfEngine &E = cached[dev];
+  if (E.capacity != cap) {
+    if (E.capacity) wf_free(E);
+    E.capacity = 0;
+    if (!wf_alloc(E, cap)) {
+      wf_free(E);
+      E.capacity = 0;
+      return RB_ERR_OUT_OF_MEMORY;
+    }
+  }
+  // the previous run synchronised its stream, so the staging table is free
+  if (njobs > E.jobs_cap) {
+    cudaFreeHost(E.h_jobs);
+    cudaFree(E.d_jobs);
+    E.h_jobs = E.d_jobs = nullptr;
+    E.jobs_cap = 0;
+    if (!cuda_ok(cudaMallocHost(&E.h_jobs, sizeof(WfJob) * njobs), "wavefront job table") ||
+        !cuda_ok(cudaMalloc(&E.d_jobs, sizeof(WfJob) * njobs), "wavefront job table"))
+      return RB_ERR_OUT_OF_MEMORY;
+    E.jobs_cap = njobs;
+  }
+  unsigned long long total = 0;
+  bool nee = false;
+  for (int j = 0; j < njobs; ++j) {
+    jobs[j].item_begin = total;
+    total += (unsigned long long)jobs[j].P.width * jobs[j].P.height * (unsigned long long)jobs[j].P.samples;
+    nee = nee || jobs[j].G.nee != 0;
+  }
+  if (total == 0) return RB_OK;
+  std::memcpy(E.h_jobs, jobs, sizeof(WfJob) * njobs);
+  WfParams W;
+  std::memset(&W, 0, sizeof W);
+  W.S = ds->view;
+  W.jobs = E.d_jobs;
+  W.njobs = njobs;
+  W.ctl = E.ctl;
+  if (ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0) {
+    if (!wf_alloc_march(E)) return RB_ERR_OUT_OF_MEMORY;
+    W.cand = E.cand;
+    W.ncand = E.ncand;
+    W.list = E.list;
+    W.cap = E.capacity;
+  }
+  cudaEvent_t fence;
+  if (!cuda_ok(cudaEventCreateWithFlags(&fence, cudaEventDisableTiming), "wavefront fence")) return RB_ERR_CUDA;
+  cudaEventRecord(fence, caller);
+  cudaStreamWaitEvent(st, fence, 0);
+  cudaMemcpyAsync(E.d_jobs, E.h_jobs, sizeof(WfJob) * njobs, cudaMemcpyHostToDevice, st);
+  WfCtl init;
+  std::memset(&init, 0, sizeof init);
+  init.total_paths = total;
+  cudaMemcpyAsync(E.ctl, &init, sizeof init, cudaMemcpyHostToDevice, st);
+  int it = 0, rc;
+  switch (ds->ms) {
+    case RB_MS_DIFFUSE: rc = nee ? wf_run<RB_MS_DIFFUSE, true>(W, E, st, &it) : wf_run<RB_MS_DIFFUSE, false>(W, E, st, &it); break;
+    case RB_MS_CLASSIC: rc = nee ? wf_run<RB_MS_CLASSIC, true>(W, E, st, &it) : wf_run<RB_MS_CLASSIC, false>(W, E, st, &it); break;
+    case RB_MS_FULL: rc = nee ? wf_run<RB_MS_FULL, true>(W, E, st, &it) : wf_run<RB_MS_FULL, false>(W, E, st, &it); break;
+    default: rc = nee ? wf_run<RB_MS_SDF, true>(W, E, st, &it) : wf_run<RB_MS_SDF, false>(W, E, st, &it); break;
+  }
+  if (rc == RB_OK && counters) {
+    counters[0] = E.h_ctl->segments;
+    counters[1] = E.h_ctl->paths_done;
+    counters[2] = E.h_ctl->overflow;
+    counters[3] = (uint64_t)it;
+  }
+  cudaEventRecord(fence, st);
+  cudaStreamWaitEvent(caller, fence, 0);
+  cudaStreamSynchronize(st);
+  cudaEventDestroy(fence);
+  return rc;
+}
+
+static WfJob wf_job(const double *frame, int width, int height, int samples, int sample_base, int max_depth,
+                    uint32_t salt, double *acc) {
+  WfJob J;
+  std::memset(&J, 0, sizeof J);
+  J.P = frame_from(frame, width, height);
+  J.P.samples = samples;
+  J.P.sample_base = sample_base;
+  J.P.max_depth = max_depth;
+  J.P.seed = current_opts().seed;
+  J.P.salt = salt;
+  J.G = current_globals();
+  J.acc = acc;
+  return J;
+}
+
 }  // namespace rb
 
 using namespace rb;
@@ -606,73 +736,36 @@ extern "C" int rb_render_wavefront(const rb_cuda_scene *scene, int width, int he
     return RB_ERR_INVALID_ARG;
   }
   if (samples == 0 || max_depth == 0) return RB_OK;
-  // The engine records its iterations into a CUDA graph, which needs a
-  // capturable stream: it runs on a private non-blocking stream ordered after
-  // the caller's stream on entry and before it on return.
+  WfJob J = wf_job(frame, width, height, samples, sample_base, max_depth, 0u, accum);
+  uint64_t c[4] = {0, 0, 0, 0};
   cudaStream_t caller = static_cast<cudaStream_t>(stream);
-  static thread_local cudaStream_t priv[64] = {nullptr};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return RB_ERR_UNSUPPORTED;
-  if (!priv[dev] && !cuda_ok(cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking), "wavefront stream"))
-    return RB_ERR_CUDA;
-  cudaStream_t st = priv[dev];
-  // queues are kept per (device, capacity) between calls: a render loop pays
-  // for their allocation once (2 x 7 arrays of capacity x 16 B)
-  const int cap = queue_capacity > 0 ? queue_capacity : (1 << 20);
-  static thread_local WfEngine cached[64];
-  WfEngine &E = cached[dev];
-  if (E.capacity != cap) {
-    if (E.capacity) wf_free(E);
-    E.capacity = 0;
-    if (!wf_alloc(E, cap)) {
-      wf_free(E);
-      E.capacity = 0;
-      return RB_ERR_OUT_OF_MEMORY;
-    }
+  const int rc = wf_render_jobs(ds, &J, 1, queue_capacity, c, caller);
+  if (rc == RB_OK && counters) cudaMemcpyAsync(counters, c, sizeof c, cudaMemcpyHostToDevice, caller);
+  return rc;
+}
+
+extern "C" int rb_render_views_wavefront(const rb_cuda_scene *scene, int n_views, int width, int height,
+                                         const double *frames, int samples, int sample_base, int max_depth,
+                                         double *accum, int queue_capacity, uint64_t *counters, void *stream) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_render_views_wavefront: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
   }
-  WfParams W;
-  std::memset(&W, 0, sizeof W);
-  W.S = ds->view;
-  W.G = current_globals();
-  W.P = frame_from(frame, width, height);
-  W.P.samples = samples;
-  W.P.sample_base = sample_base;
-  W.P.max_depth = max_depth;
-  W.P.seed = current_opts().seed;
-  W.P.salt = 0;
-  W.acc = accum;
-  W.ctl = E.ctl;
-  if (ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0) {
-    if (!wf_alloc_march(E)) return RB_ERR_OUT_OF_MEMORY;
-    W.cand = E.cand;
-    W.ncand = E.ncand;
-    W.list = E.list;
-    W.cap = E.capacity;
+  if (n_views <= 0 || n_views > 4096 || width <= 0 || height <= 0 || !frames || !accum || samples < 0 ||
+      max_depth < 0 || sample_base < 0) {
+    set_error("rb_render_views_wavefront: invalid argument");
+    return RB_ERR_INVALID_ARG;
   }
-  cudaEvent_t fence;
-  if (!cuda_ok(cudaEventCreateWithFlags(&fence, cudaEventDisableTiming), "wavefront fence")) return RB_ERR_CUDA;
-  cudaEventRecord(fence, caller);
-  cudaStreamWaitEvent(st, fence, 0);
-  WfCtl init;
-  std::memset(&init, 0, sizeof init);
-  init.total_paths = (unsigned long long)width * height * samples;
-  cudaMemcpyAsync(E.ctl, &init, sizeof init, cudaMemcpyHostToDevice, st);
-  int it = 0, rc;
-  const bool nee = W.G.nee != 0;
-  switch (ds->ms) {
-    case RB_MS_DIFFUSE: rc = nee ? wf_run<RB_MS_DIFFUSE, true>(W, E, st, &it) : wf_run<RB_MS_DIFFUSE, false>(W, E, st, &it); break;
-    case RB_MS_CLASSIC: rc = nee ? wf_run<RB_MS_CLASSIC, true>(W, E, st, &it) : wf_run<RB_MS_CLASSIC, false>(W, E, st, &it); break;
-    case RB_MS_FULL: rc = nee ? wf_run<RB_MS_FULL, true>(W, E, st, &it) : wf_run<RB_MS_FULL, false>(W, E, st, &it); break;
-    default: rc = nee ? wf_run<RB_MS_SDF, true>(W, E, st, &it) : wf_run<RB_MS_SDF, false>(W, E, st, &it); break;
-  }
-  if (rc == RB_OK && counters) {
-    uint64_t c[4] = {E.h_ctl->segments, E.h_ctl->paths_done, E.h_ctl->overflow, (uint64_t)it};
-    cudaMemcpyAsync(counters, c, sizeof c, cudaMemcpyHostToDevice, st);
-  }
-  cudaEventRecord(fence, st);
-  cudaStreamWaitEvent(caller, fence, 0);
-  cudaStreamSynchronize(st);
-  cudaEventDestroy(fence);
+  if (samples == 0 || max_depth == 0) return RB_OK;
+  std::vector<WfJob> jobs((size_t)n_views);
+  const size_t npx = (size_t)width * height;
+  for (int v = 0; v < n_views; ++v)
+    jobs[v] = wf_job(frames + 21 * (size_t)v, width, height, samples, sample_base, max_depth, (uint32_t)v,
+                     accum + 4 * npx * v);
+  uint64_t c[4] = {0, 0, 0, 0};
+  cudaStream_t caller = static_cast<cudaStream_t>(stream);
+  const int rc = wf_render_jobs(ds, jobs.data(), n_views, queue_capacity, c, caller);
+  if (rc == RB_OK && counters) cudaMemcpyAsync(counters, c, sizeof c, cudaMemcpyHostToDevice, caller);
   return rc;
 }

@@ -149,6 +149,27 @@ def render_views(ds, frames, w: int, h: int, spp: int, depth: int, background: f
     return (img, cnt.cpu().numpy()) if counters else img
 
 
+def render_views_wavefront(ds, frames, w: int, h: int, spp: int, depth: int, background: float = 1.0,
+                           dof: tuple | None = None, nee: bool = False, sample_base: int = 0,
+                           seed: int = DEFAULT_SEED, queue_capacity: int = 0, counters: bool = False):
+    """Per-view radiance sums (n_views, h, w, 3) float64 of several camera frames
+    rendered by one wavefront run over all views (rb_render_views_wavefront)."""
+    torch = _torch()
+    fr = np.ascontiguousarray(np.stack([np.asarray(f, np.float64) for f in frames]))
+    n = fr.shape[0]
+    set_globals(background=background, dof=dof)
+    acc = torch.zeros((n, w * h, 4), dtype=torch.float64, device="cuda")
+    cnt = torch.zeros(4, dtype=torch.int64, device="cuda")
+    with options(nee=nee, seed=seed):
+        check(lib.rb_render_views_wavefront(ds.handle, n, w, h, fr.ctypes.data_as(C.POINTER(C.c_double)), spp,
+                                            sample_base, depth, C.c_void_p(acc.data_ptr()), int(queue_capacity),
+                                            C.c_void_p(cnt.data_ptr()), _stream_ptr()), "rb_render_views_wavefront")
+        torch.cuda.synchronize()
+    set_globals()
+    img = acc[:, :, :3].cpu().numpy().reshape(n, h, w, 3)
+    return (img, cnt.cpu().numpy()) if counters else img
+
+
 def render_dropin(ds, frame, w: int, h: int, spp: int, depth: int, chunks: int = 5):
     """RendererCUDA::render's loop (renderer_cuda_host.hpp:35-58) through the drop-in
     entry point with a host float3 accumulation buffer. Returns (h, w, 3) float32 sums."""

@@ -146,3 +146,32 @@ def test_trace_latencies(cuda):
     assert st.jobs_done == 30 and st.p99_latency >= st.p50_latency > 0
     assert st.paths == sum(r.width * r.height * r.spp for r in reqs)
     srv.close()
+
+
+def test_sdf_field_jobs_on_the_wavefront_engine(cuda):
+    # jobs of a smooth-SDF scene run on the wavefront engine (FP64
+    # accumulation); the same job through the batched kernel and the
+    # per-frame kernel (salt 0 = the job's seed 0) draws the same streams
+    spec = scenes.sdf_field(count=48, width=48, height=32)
+    w, h, spp = 48, 32, 16
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = spec.camera.frame(w, h)
+    out = {}
+    for wf in (True, False):
+        srv = serving.Server(paths_per_iteration=w * h * 8, max_spp_per_iteration=8, wavefront_field=wf)
+        sid = srv.add_scene(ds)
+        j = srv.submit(serving.job(sid, fr, w, h, spp, spec.depth, background=spec.background, seed=0))
+        srv.drain()
+        st = srv.status(j)
+        assert st.state == 2 and st.spp_done == spp
+        out[wf] = srv.fetch(j, w, h)
+        assert srv.stats().paths == w * h * spp
+        srv.close()
+    ref = render.render_accumulate(ds, fr, w, h, spp, spec.depth, background=spec.background)
+    for got in out.values():
+        bad = (np.abs(got - ref) > 2e-3 * (1 + np.abs(ref)) * spp).any(axis=2)
+        assert bad.mean() < 0.04, bad.mean()
+        np.testing.assert_allclose(got.mean((0, 1)), ref.mean((0, 1)), rtol=2e-2, atol=1e-3)
+    ds.free()

@@ -59,3 +59,24 @@ def test_views_accumulate_and_reject_bad_arguments(cuda):
                                  4, C.c_void_p(acc.data_ptr()), None, None)
         assert st < 0
     ds.free()
+
+
+@pytest.mark.parametrize("name", ["cornell", "sdf_field"])
+def test_views_wavefront_paired_with_views_kernel(cuda, name):
+    # one wavefront run over all views draws the same streams (view v on salt
+    # v) as the batched kernel; the paths agree except where FP32 marching or
+    # accumulation order branches a path differently
+    spec = scenes.sdf_field(count=48) if name == "sdf_field" else scenes.cornell()
+    w, h, spp, n = 48, 32, 8, 4
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    frames = _orbit_frames(spec, n, w, h)
+    a = render.render_views(ds, frames, w, h, spp, spec.depth, background=spec.background)
+    b, cnt = render.render_views_wavefront(ds, frames, w, h, spp, spec.depth, background=spec.background,
+                                           queue_capacity=2048, counters=True)
+    assert int(cnt[1]) == n * w * h * spp
+    bad = (np.abs(a - b) > 2e-3 * (1 + np.abs(a)) * spp).any(axis=3)
+    assert bad.mean() < 0.04, bad.mean()
+    np.testing.assert_allclose(a.mean((1, 2)), b.mean((1, 2)), rtol=2e-2, atol=1e-3)
+    ds.free()
