@@ -481,10 +481,9 @@ __device__ __forceinline__ float sdf_eval1(const SdfPrim &q, const f3 &pw) {
   }
 }
 
-// sdf_eval1 of primitive i of the table, its record read as five 128-bit loads.
-__device__ __forceinline__ float sdf_eval_at(const SdfPrim *__restrict__ tab, int i, const f3 &pw) {
-  const float4 *v = reinterpret_cast<const float4 *>(tab + i);
-  const float4 w0 = __ldg(v), w1 = __ldg(v + 1), w2 = __ldg(v + 2), w3 = __ldg(v + 3), w4 = __ldg(v + 4);
+// sdf_eval1 of a record given as its five 16-byte words.
+__device__ __forceinline__ float sdf_eval_words(const float4 &w0, const float4 &w1, const float4 &w2, const float4 &w3,
+                                                const float4 &w4, const f3 &pw) {
   SdfPrim q;
   q.px = w0.x; q.py = w0.y; q.pz = w0.z; q.a = w0.w;
   q.b = w1.x; q.c = w1.y; q.round = w1.z; q.type = __float_as_int(w1.w);
@@ -492,6 +491,12 @@ __device__ __forceinline__ float sdf_eval_at(const SdfPrim *__restrict__ tab, in
   q.r11 = w3.x; q.r12 = w3.y; q.r20 = w3.z; q.r21 = w3.w;
   q.r22 = w4.x;
   return sdf_eval1(q, pw);
+}
+
+// sdf_eval1 of primitive i of the table, its record read as five 128-bit loads.
+__device__ __forceinline__ float sdf_eval_at(const SdfPrim *__restrict__ tab, int i, const f3 &pw) {
+  const float4 *v = reinterpret_cast<const float4 *>(tab + i);
+  return sdf_eval_words(__ldg(v), __ldg(v + 1), __ldg(v + 2), __ldg(v + 3), __ldg(v + 4), pw);
 }
 
 __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {

@@ -177,14 +177,18 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi
 struct WfFold {
   float F = RB_SDF_FAR, best = RB_SDF_FAR, next = RB_SDF_FAR;
   bool first = true;
-  __device__ __forceinline__ void add(const SceneView &S, const int4 e, const f3 &p, float t, int *nearest) {
+  // tab: the SDF table staged in shared memory (5 words per record), or null
+  __device__ __forceinline__ void add(const SceneView &S, const float4 *tab, const int4 e, const f3 &p, float t,
+                                      int *nearest) {
     const float t0 = __int_as_float(e.y);
     if (t0 > t) {
       next = fminf(next, t0);
       return;
     }
     if (t > __int_as_float(e.z)) return;
-    const float d = sdf_eval_at(S.sdf, e.x, p);
+    const float d = tab ? sdf_eval_words(tab[5 * e.x], tab[5 * e.x + 1], tab[5 * e.x + 2], tab[5 * e.x + 3],
+                                         tab[5 * e.x + 4], p)
+                        : sdf_eval_at(S.sdf, e.x, p);
     if (nearest && d < best) {
       best = d;
       *nearest = e.x;
@@ -194,14 +198,14 @@ struct WfFold {
   }
 };
 
-__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, int slot, int n,
+__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, const float4 *tab, int slot, int n,
                                           const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
                                           int *nearest) {
   WfFold f;
 #pragma unroll
   for (int i = 0; i < WF_CAND_REG; ++i)
-    if (i < n) f.add(S, cr[i], p, t, nearest);
-  for (int i = WF_CAND_REG; i < n; ++i) f.add(S, __ldg(W.cand + (size_t)i * W.cap + slot), p, t, nearest);
+    if (i < n) f.add(S, tab, cr[i], p, t, nearest);
+  for (int i = WF_CAND_REG; i < n; ++i) f.add(S, tab, __ldg(W.cand + (size_t)i * W.cap + slot), p, t, nearest);
   next = f.next;
   return f.F;
 }
@@ -219,9 +223,17 @@ __device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W,
 enum : int { WF_ESCAPE = 0, WF_MARCH = 1, WF_NORMAL = 2 };
 
 template <int MS>
-__global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q) {
+__global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int stage_table) {
+  extern __shared__ float4 s_tab[];
   const int lane = threadIdx.x & 31;
   const SceneView &S = W.S;
+  // stage the SDF table in shared memory when it fits (stage_table != 0)
+  if (stage_table) {
+    const float4 *g = reinterpret_cast<const float4 *>(S.sdf);
+    for (int i = threadIdx.x; i < 5 * S.num_sdf; i += blockDim.x) s_tab[i] = __ldg(g + i);
+    __syncthreads();
+  }
+  const float4 *tab = stage_table ? s_tab : nullptr;
   const unsigned total = (unsigned)W.ctl->march_count;
   const float e = RB_SDF_NORMAL_EPS;
   int slot = 0, n = 0, steps = 0, phase = WF_ESCAPE, sub = 0, nearest = 0;
@@ -278,7 +290,7 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q) {
     }
     float next;
     int near = cr[0].x;
-    const float raw = wf_field(S, W, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near);
+    const float raw = wf_field(S, W, tab, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near);
     bool finished = false;
     if (phase == WF_NORMAL) {
       if (sub & 1) {
@@ -564,12 +576,24 @@ static bool wf_alloc(WfEngine &E, int capacity) {
   return ok;
 }
 
+// Shared-memory bytes of the staged SDF table (0 when it does not fit in 48 KB).
+#ifndef WF_STAGE_SDF_TABLE
+#define WF_STAGE_SDF_TABLE 1
+#endif
+static size_t wf_table_bytes(const WfParams &W) {
+  const size_t b = sizeof(SdfPrim) * (size_t)W.S.num_sdf;
+  return b <= 48 * 1024 ? b : 0;
+}
+
 template <int MS, bool NEE>
 static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int march_grid, cudaStream_t st) {
   const size_t sm = sizeof(int2) * RB_SHORT * 256;
   k_wf_reset<<<1, 1, 0, st>>>(E.ctl, qi ^ 1);
   k_wf_extend<MS><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
-  if (march_grid > 0) k_wf_march<MS><<<march_grid, 256, 0, st>>>(W, E.q[qi]);
+  if (march_grid > 0) {
+    const size_t tab = WF_STAGE_SDF_TABLE ? wf_table_bytes(W) : 0;
+    k_wf_march<MS><<<march_grid, 256, tab, st>>>(W, E.q[qi], tab > 0 ? 1 : 0);
+  }
   k_wf_shade<MS, NEE><<<grid, 256, sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
 }
 
@@ -579,7 +603,8 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   int march_grid = 0;
   if (MS >= RB_MS_SDF && W.cand) {  // persistent march: the resident blocks
     int per_sm = 0, dev = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS>, 256,
+                                                  WF_STAGE_SDF_TABLE ? wf_table_bytes(W) : 0);
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     march_grid = std::max(1, per_sm) * sms;
