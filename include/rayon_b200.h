@@ -170,6 +170,16 @@ int64_t rb_scene_add_spheres(rb_scene_desc *s, const double *cr, const int32_t *
                              int mat_id, int64_t n);
 int64_t rb_scene_add_triangles(rb_scene_desc *s, const double *v, const double *nrm,
                                const int32_t *mat_ids, int mat_id, int64_t n);
+/* Wavefront OBJ mesh (replaces Scene::OBJLoader::loadOBJ,
+ * src/rayon/scenes/obj_loader.hpp:34-140, with its semantics: positions
+ * scaled then translated, fan triangulation, 1-based and negative indices,
+ * vertex normals only when all three are valid, invalid triangles skipped).
+ * position / scale may be NULL (0 and 1). Returns the number of triangles
+ * added, RB_ERR_NOT_FOUND when the file cannot be opened, RB_ERR_INVALID_ARG
+ * on a malformed face index (where the reference throws; triangles of earlier
+ * faces stay added). */
+int64_t rb_scene_load_obj(rb_scene_desc *s, const char *path, int mat_id, const double position[3],
+                          const double scale[3]);
 int rb_scene_set_visible(rb_scene_desc *s, int64_t geom_index, int visible);
 int64_t rb_scene_num_geometries(const rb_scene_desc *s);
 int rb_scene_num_materials(const rb_scene_desc *s);

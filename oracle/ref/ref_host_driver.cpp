@@ -22,6 +22,7 @@
 #include "rayon_b200_scene.h"
 #include "render/renderer_interface.hpp"
 #include "renderer_cpu_parallel.hpp"
+#include "obj_loader.hpp"
 #include "scene_description.hpp"
 
 using Scene::SceneDescription;
@@ -79,6 +80,25 @@ int refh_add_geoms(void *sp, const uint8_t *kinds, const double *params, const i
     stash(s->geometries.back(), (int64_t)s->geometries.size() - 1);
   }
   return 0;
+}
+
+// The reference's OBJ loader (obj_loader.hpp:34-140) into the scene; returns its count or -1.
+int refh_load_obj(void *sp, const char *path, int mat, const double *pos, const double *scale) {
+  return Scene::OBJLoader::loadOBJ(path, *static_cast<SceneDescription *>(sp), mat, v3(pos), v3(scale));
+}
+int64_t refh_num_geoms(void *sp) { return (int64_t) static_cast<SceneDescription *>(sp)->geometries.size(); }
+// Triangles in insertion order: v0 v1 v2 n0 n1 n2 (18 doubles), has_normals, material.
+void refh_export_triangles(void *sp, double *out) {
+  const auto &g = static_cast<SceneDescription *>(sp)->geometries;
+  for (size_t i = 0; i < g.size(); ++i) {
+    double *o = out + 20 * i;
+    const auto &t = g[i].data.triangle;
+    const Vec3 *v[6] = {&t.v0, &t.v1, &t.v2, &t.n0, &t.n1, &t.n2};
+    for (int k = 0; k < 6; ++k)
+      for (int c = 0; c < 3; ++c) o[3 * k + c] = (*v[k])[c];
+    o[18] = t.has_normals ? 1.0 : 0.0;
+    o[19] = (double)g[i].material_id;
+  }
 }
 
 void refh_build_bvh(void *sp) { static_cast<SceneDescription *>(sp)->buildBVH(); }

@@ -47,6 +47,11 @@ def host():
         L.refh_export_bvh.argtypes = [vp, dp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint8),
                                       C.POINTER(C.c_uint8)]
         L.refh_export_order.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.refh_load_obj.argtypes = [vp, C.c_char_p, C.c_int, dp, dp]
+        L.refh_load_obj.restype = C.c_int
+        L.refh_num_geoms.argtypes = [vp]
+        L.refh_num_geoms.restype = C.c_int64
+        L.refh_export_triangles.argtypes = [vp, dp]
         L.refh_render_cpu_parallel.restype = C.c_double
         L.refh_render_cpu_parallel.argtypes = [vp, dp, dp, dp, C.c_double, C.c_int, C.c_int, C.c_int,
                                                C.POINTER(C.c_uint8), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
@@ -102,3 +107,22 @@ class RefScene:
         if getattr(self, "h", None):
             self.L.refh_scene_destroy(self.h)
             self.h = None
+
+
+def reference_obj_triangles(path, mat: int, position=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0)):
+    """Loads an OBJ file with the reference's own OBJLoader::loadOBJ into a
+    fresh reference SceneDescription; returns (count, n x 20 array: v0 v1 v2
+    n0 n1 n2, has_normals, material) in insertion order."""
+    import numpy as np
+    L = host()
+    sp = L.refh_scene_create()
+    try:
+        pos = (C.c_double * 3)(*position)
+        sc = (C.c_double * 3)(*scale)
+        n = L.refh_load_obj(sp, str(path).encode(), int(mat), pos, sc)
+        g = int(L.refh_num_geoms(sp))
+        out = np.zeros((g, 20), np.float64)
+        L.refh_export_triangles(sp, out.ctypes.data_as(dp))
+        return n, out
+    finally:
+        L.refh_scene_destroy(sp)

@@ -120,6 +120,7 @@ _sig("rb_scene_add_triangle_with_normals", C.c_int, vp, c_double_p, c_double_p, 
 _sig("rb_scene_add_sdf", C.c_int, vp, C.c_int, c_double_p, c_double_p, c_double_p, C.c_int)
 _sig("rb_scene_add_spheres", C.c_int64, vp, c_double_p, c_int32_p, C.c_int, C.c_int64)
 _sig("rb_scene_add_triangles", C.c_int64, vp, c_double_p, c_double_p, c_int32_p, C.c_int, C.c_int64)
+_sig("rb_scene_load_obj", C.c_int64, vp, C.c_char_p, C.c_int, c_double_p, c_double_p)
 _sig("rb_scene_set_visible", C.c_int, vp, C.c_int64, C.c_int)
 _sig("rb_scene_num_geometries", C.c_int64, vp)
 _sig("rb_scene_num_materials", C.c_int, vp)

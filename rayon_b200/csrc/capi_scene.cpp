@@ -117,6 +117,20 @@ int64_t rb_scene_add_triangles(rb_scene_desc *s, const double *v, const double *
   return first;
 }
 
+int64_t rb_scene_load_obj(rb_scene_desc *s, const char *path, int mat_id, const double position[3],
+                          const double scale[3]) {
+  if (!s || !path) return RB_ERR_INVALID_ARG;
+  const V3 pos = position ? v3(position) : V3(0, 0, 0);
+  const V3 sc = scale ? v3(scale) : V3(1, 1, 1);
+  std::string err;
+  const int64_t n = rb::load_obj(s->s, path, mat_id, pos, sc, err);
+  if (n < 0) {
+    rb::set_error("rb_scene_load_obj: " + err);
+    return err.rfind("cannot open", 0) == 0 ? RB_ERR_NOT_FOUND : RB_ERR_INVALID_ARG;
+  }
+  return n;
+}
+
 int rb_scene_set_visible(rb_scene_desc *s, int64_t i, int visible) {
   // i is the insertion index (the index an add call returned), also after a
   // BVH build has permuted the geometries to leaf order.

@@ -88,6 +88,10 @@ class HostScene {
   bool build_bvh(int max_leaf, int threads);
 };
 
+// Wavefront OBJ file into the scene with OBJLoader::loadOBJ's semantics
+// (obj_ingest.cpp); returns the triangles added, or -1 with err set.
+int64_t load_obj(HostScene &hs, const char *path, int mat, const V3 &pos, const V3 &scale, std::string &err);
+
 // Radius of a sphere around an SDF primitive's position that contains it.
 double sdf_bound_radius(const Geom &g);
 

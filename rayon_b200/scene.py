@@ -163,6 +163,11 @@ class SceneDescription:
                                                 None if mids is None else mids.ctypes.data_as(c_int32_p),
                                                 int(mat_id), v.shape[0]), "add_triangles")
 
+    def load_obj(self, path, mat_id: int, position=(0.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0)) -> int:
+        """Triangles of a Wavefront OBJ file (OBJLoader::loadOBJ semantics); returns their count."""
+        return check(lib.rb_scene_load_obj(self._h, str(path).encode(), int(mat_id), _d3(position), _d3(scale)),
+                     "load_obj")
+
     def set_visible(self, geom_index: int, visible: bool) -> None:
         check(lib.rb_scene_set_visible(self._h, int(geom_index), int(bool(visible))), "set_visible")
 
