@@ -349,7 +349,12 @@ typedef struct rb_server_opts {
   int occupancy;                /* resident 256-thread blocks per SM (0 = tuned) */
   int wavefront_field;          /* 1 (default): jobs of scenes with a smooth SDF field run on the
                                    wavefront engine (FP64 accumulation); 0: batched kernel */
-  int reserved[2];
+  float target_iteration_ms;    /* > 0: latency-target controller. After each iteration the path
+                                   quantum is scaled by clamp(target / measured, 0.5, 2) within
+                                   [2^18, paths_per_iteration], the rule of the progressive
+                                   renderer's batch controller (renderer_cuda_progressive_host.hpp:
+                                   677-685) applied to the server's quantum. 0: fixed quantum */
+  int reserved[1];
 } rb_server_opts;
 
 void rb_server_default_opts(rb_server_opts *out);
@@ -368,6 +373,8 @@ typedef struct rb_server_stats {
   double wall_seconds;     /* first arrival to last completion */
   int64_t peak_device_bytes;
   double p50_latency, p99_latency, mean_latency;  /* arrival -> done, seconds */
+  int64_t quantum_paths;      /* path quantum of the next iteration */
+  double last_iteration_ms;   /* device time of the last iteration */
 } rb_server_stats;
 
 typedef struct rb_server rb_server;

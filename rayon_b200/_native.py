@@ -174,7 +174,8 @@ class JobRequest(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_int64), ("max_active_jobs", C.c_int), ("paths_per_iteration", C.c_int64),
                 ("max_spp_per_iteration", C.c_int), ("use_graph", C.c_int), ("frames_every", C.c_int),
-                ("occupancy", C.c_int), ("wavefront_field", C.c_int), ("reserved", C.c_int * 2)]
+                ("occupancy", C.c_int), ("wavefront_field", C.c_int), ("target_iteration_ms", C.c_float),
+                ("reserved", C.c_int * 1)]
 
 
 class JobStatus(C.Structure):
@@ -186,7 +187,8 @@ class ServerStats(C.Structure):
     _fields_ = [("jobs_done", C.c_int64), ("jobs_rejected", C.c_int64), ("iterations", C.c_int64),
                 ("frames", C.c_int64), ("paths", C.c_int64), ("segments", C.c_int64),
                 ("device_seconds", C.c_double), ("wall_seconds", C.c_double), ("peak_device_bytes", C.c_int64),
-                ("p50_latency", C.c_double), ("p99_latency", C.c_double), ("mean_latency", C.c_double)]
+                ("p50_latency", C.c_double), ("p99_latency", C.c_double), ("mean_latency", C.c_double),
+                ("quantum_paths", C.c_int64), ("last_iteration_ms", C.c_double)]
 
 
 _sig("rb_job_default", None, C.POINTER(JobRequest))

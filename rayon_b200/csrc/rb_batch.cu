@@ -288,6 +288,8 @@ struct Server {
   rb_server_stats stats;
   std::vector<double> latencies;
   double first_arrival = -1, last_done = 0;
+  int64_t quantum = 0;        // path quantum of the next iteration
+  double last_ms = 0.0;       // device time of the last iteration
 
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -383,7 +385,7 @@ static int server_step(Server &S) {
     cand.push_back({id, 0, cls, rem / (1.0 + S.aging * age)});
   }
   std::stable_sort(cand.begin(), cand.end(), [](const Plan &a, const Plan &b) { return a.prio < b.prio; });
-  int64_t budget = S.o.paths_per_iteration;
+  int64_t budget = S.quantum > 0 ? S.quantum : S.o.paths_per_iteration;
   std::vector<Plan> plan;
   for (Plan &c : cand) {
     if (budget <= 0 && !plan.empty()) break;
@@ -534,6 +536,14 @@ static int server_step(Server &S) {
   float ms_it = 0.f;
   cudaEventElapsedTime(&ms_it, S.ev0, S.ev1);
   S.stats.device_seconds += ms_it * 1e-3;
+  S.last_ms = ms_it;
+  // latency-target controller: the quantum follows the measured iteration time
+  // (only when the iteration used its whole quantum; a short queue says nothing)
+  if (S.o.target_iteration_ms > 0.0f && ms_it > 0.0f && budget <= 0) {
+    const double scale = std::min(2.0, std::max(0.5, (double)S.o.target_iteration_ms / (double)ms_it));
+    const int64_t q = (int64_t)std::llround((double)S.quantum * scale);
+    S.quantum = std::min<int64_t>(S.o.paths_per_iteration, std::max<int64_t>(int64_t(1) << 18, q));
+  }
   S.stats.iterations++;
   for (int c = 1; c < RB_GROUPS; ++c) {
     S.stats.paths += (int64_t)S.h_ctl[c].paths;
@@ -632,6 +642,7 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   cudaEventCreate(&S.ev0);
   cudaEventCreate(&S.ev1);
   std::memset(&S.stats, 0, sizeof S.stats);
+  S.quantum = S.o.paths_per_iteration;
   S.t0 = std::chrono::steady_clock::now();
   return r;
 }
@@ -801,6 +812,8 @@ int rb_server_get_stats(rb_server *r, rb_server_stats *out) {
   Server &S = r->s;
   *out = S.stats;
   out->peak_device_bytes = S.peak_bytes;
+  out->quantum_paths = S.quantum;
+  out->last_iteration_ms = S.last_ms;
   out->wall_seconds = S.first_arrival >= 0 ? S.last_done - S.first_arrival : 0.0;
   std::vector<double> l = S.latencies;
   if (!l.empty()) {

@@ -26,7 +26,7 @@ def job(scene: int, frame, width: int, height: int, spp: int, depth: int, backgr
 class Server:
     def __init__(self, budget_bytes: int | None = None, max_jobs: int | None = None, paths_per_iteration=None,
                  max_spp_per_iteration=None, use_graph: bool = True, frames_every: int = 0, occupancy: int = 0,
-                 wavefront_field: bool = True, stream=None):
+                 wavefront_field: bool = True, target_iteration_ms: float = 0.0, stream=None):
         o = ServerOpts()
         lib.rb_server_default_opts(C.byref(o))
         if budget_bytes is not None:
@@ -39,6 +39,7 @@ class Server:
             o.max_spp_per_iteration = int(max_spp_per_iteration)
         o.use_graph, o.frames_every, o.occupancy = int(use_graph), int(frames_every), int(occupancy)
         o.wavefront_field = int(wavefront_field)
+        o.target_iteration_ms = float(target_iteration_ms)
         self.h = lib.rb_server_create(C.byref(o), stream)
         if not self.h:
             raise RuntimeError(lib.rb_last_error().decode())

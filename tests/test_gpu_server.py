@@ -175,3 +175,28 @@ def test_sdf_field_jobs_on_the_wavefront_engine(cuda):
         assert bad.mean() < 0.04, bad.mean()
         np.testing.assert_allclose(got.mean((0, 1)), ref.mean((0, 1)), rtol=2e-2, atol=1e-3)
     ds.free()
+
+
+def test_latency_target_controller(cuda):
+    # the path quantum follows clamp(target / measured, 0.5, 2) per full
+    # iteration: from a 64 M-path quantum it settles where an iteration takes
+    # about the target time
+    spec = scenes.cornell()
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    target = 4.0
+    srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=1024, target_iteration_ms=target)
+    sid = srv.add_scene(ds)
+    fr = spec.camera.frame(512, 512)
+    ms = []
+    for k in range(6):
+        srv.submit(serving.job(sid, fr, 512, 512, 1024, spec.depth, background=0.0, seed=k))
+    while srv.step() > 0:
+        ms.append(srv.stats().last_iteration_ms)
+    st = srv.stats()
+    assert st.quantum_paths < 64 << 20
+    tail = ms[len(ms) // 2:-2]  # settled iterations (the last ones drain the queue)
+    assert tail and 0.4 * target < float(np.median(tail)) < 2.5 * target, ms
+    srv.close()
+    ds.free()
