@@ -334,6 +334,16 @@ typedef struct rb_job_request {
   uint32_t seed;         /* job key of the counter-based sample streams */
   int fp64_accum;        /* 1: FP64 accumulation (always used above 65536 spp) */
   double arrival_time;   /* seconds on the server clock (rb_server_run_trace) */
+  /* Per-job convergence (0 = off): after each iteration that gave the job
+   * samples, a pixel counts as converged when, with at least
+   * converge_min_spp samples, its mean luminance changed by less than
+   * converge_threshold relative to the new mean (the per-pixel test of
+   * render_acc_kernel.cu:241-271) and stays converged; the job completes
+   * early when at least converge_fraction of its pixels are converged. */
+  float converge_threshold;
+  int converge_min_spp;
+  float converge_fraction;
+  int converge_pad;
 } rb_job_request;
 
 /* Defaults for rb_job_request: the reference's __constant__ shading values. */

@@ -168,7 +168,9 @@ class JobRequest(C.Structure):
                 ("max_depth", C.c_int), ("frame", C.c_double * 21), ("light_intensity", C.c_float),
                 ("background_intensity", C.c_float), ("metal_fuzziness", C.c_float), ("glass_ior", C.c_float),
                 ("dof_enabled", C.c_int), ("dof_aperture", C.c_float), ("dof_focus", C.c_float), ("nee", C.c_int),
-                ("seed", C.c_uint32), ("fp64_accum", C.c_int), ("arrival_time", C.c_double)]
+                ("seed", C.c_uint32), ("fp64_accum", C.c_int), ("arrival_time", C.c_double),
+                ("converge_threshold", C.c_float), ("converge_min_spp", C.c_int), ("converge_fraction", C.c_float),
+                ("converge_pad", C.c_int)]
 
 
 class ServerOpts(C.Structure):

@@ -262,6 +262,8 @@ struct Job {
   float4 *acc = nullptr;
   double *acc64 = nullptr;
   unsigned char *frame = nullptr;
+  float *lum = nullptr;       // mean luminance at the last convergence check (converging jobs)
+  bool converged = false;
   int64_t bytes = 0;
 };
 
@@ -280,6 +282,7 @@ struct Server {
   BatchJob *d_jobs = nullptr;
   BatchCtl *h_ctl = nullptr;   // pinned
   BatchCtl *d_ctl = nullptr;
+  unsigned long long *h_conv = nullptr, *d_conv = nullptr;  // converged-pixel counts per planned job
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_frames = -1;
@@ -296,8 +299,40 @@ struct Server {
 
 static int64_t job_bytes(const rb_job_request &r, bool frames) {
   const int64_t n = (int64_t)r.width * r.height;
-  const bool f64 = r.fp64_accum || r.spp > 65536;
-  return (f64 ? n * 32 : n * 32) + (frames ? n * 4 : 0);
+  return n * 32 + (frames ? n * 4 : 0) + (r.converge_threshold > 0.0f ? n * 4 : 0);
+}
+
+// Per-job convergence count: the per-pixel luminance test of the reference's
+// adaptive sampling (render_acc_kernel.cu:241-271) between the job's last
+// check (lum) and its sums now (spp_now samples). As in the reference a
+// converged pixel stays converged: lum holds -1 - (its luminance) from then
+// on (the reference keeps the flag in the sign of its sample count). Counts
+// the converged pixels.
+__global__ void k_job_converge(const float4 *__restrict__ acc, const double *__restrict__ acc64, float *lum, int n,
+                               int spp_now, int checked_before, float threshold, unsigned long long *count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool conv = false;
+  if (i < n) {
+    float r, g, b;
+    if (acc64) {
+      const double4 v = reinterpret_cast<const double4 *>(acc64)[i];
+      r = (float)v.x; g = (float)v.y; b = (float)v.z;
+    } else {
+      const float4 a = acc[i], c = acc[n + i];
+      r = a.x - c.x; g = a.y - c.y; b = a.z - c.z;
+    }
+    const float lum_before = lum[i];
+    if (lum_before < 0.0f) {
+      conv = true;
+    } else {
+      const float inv_s = 1.0f / (float)spp_now;
+      const float lum_after = 0.299f * r * inv_s + 0.587f * g * inv_s + 0.114f * b * inv_s;
+      conv = checked_before && fabsf(lum_after - lum_before) / fmaxf(lum_after, 0.001f) < threshold;
+      lum[i] = conv ? -1.0f - lum_after : lum_after;
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, conv);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
 }
 
 // Jobs of scenes with a smooth SDF field run on the wavefront engine, whose
@@ -327,12 +362,17 @@ static bool admit(Server &S, Job &J) {
     e = cudaMallocAsync((void **)&J.frame, n * 4, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.frame, 0, n * 4, S.st);
   }
+  if (e == cudaSuccess && J.req.converge_threshold > 0.0f) {
+    e = cudaMallocAsync((void **)&J.lum, n * 4, S.st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(J.lum, 0, n * 4, S.st);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     if (J.acc) cudaFreeAsync(J.acc, S.st);
     if (J.acc64) cudaFreeAsync(J.acc64, S.st);
     if (J.frame) cudaFreeAsync(J.frame, S.st);
-    J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr;
+    if (J.lum) cudaFreeAsync(J.lum, S.st);
+    J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr; J.lum = nullptr;
     return false;
   }
   J.bytes = need;
@@ -348,7 +388,8 @@ static void free_job(Server &S, Job &J) {
   if (J.acc) cudaFreeAsync(J.acc, S.st);
   if (J.acc64) cudaFreeAsync(J.acc64, S.st);
   if (J.frame) cudaFreeAsync(J.frame, S.st);
-  J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr;
+  if (J.lum) cudaFreeAsync(J.lum, S.st);
+  J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr; J.lum = nullptr;
   S.used_bytes -= J.bytes;
   J.bytes = 0;
 }
@@ -552,6 +593,32 @@ static int server_step(Server &S) {
   S.stats.paths += (int64_t)wf_paths;
   S.stats.segments += (int64_t)wf_segments;
   if (frames) S.stats.frames += (int64_t)plan.size();
+  // per-job convergence of the jobs that asked for it
+  {
+    std::vector<size_t> conv_k;
+    for (size_t k = 0; k < plan.size(); ++k)
+      if (S.jobs[plan[k].id].req.converge_threshold > 0.0f) conv_k.push_back(k);
+    if (!conv_k.empty()) {
+      cudaMemsetAsync(S.d_conv, 0, sizeof(unsigned long long) * conv_k.size(), S.st);
+      for (size_t c = 0; c < conv_k.size(); ++c) {
+        Job &J = S.jobs[plan[conv_k[c]].id];
+        const int n = J.req.width * J.req.height;
+        const int spp_now = J.spp_done + plan[conv_k[c]].spp;
+        const int checked = J.spp_done > 0 && spp_now >= J.req.converge_min_spp ? 1 : 0;
+        k_job_converge<<<(n + 255) / 256, 256, 0, S.st>>>(J.acc, J.acc64, J.lum, n, spp_now, checked,
+                                                          J.req.converge_threshold, S.d_conv + c);
+        g_launches++;
+      }
+      cudaMemcpyAsync(S.h_conv, S.d_conv, sizeof(unsigned long long) * conv_k.size(), cudaMemcpyDeviceToHost,
+                      S.st);
+      if (!cuda_ok(cudaStreamSynchronize(S.st), "job convergence")) return RB_ERR_CUDA;
+      for (size_t c = 0; c < conv_k.size(); ++c) {
+        Job &J = S.jobs[plan[conv_k[c]].id];
+        const double n = (double)J.req.width * J.req.height;
+        if ((double)S.h_conv[c] >= (double)J.req.converge_fraction * n) J.converged = true;
+      }
+    }
+  }
   // retire
   const double t = S.now();
   std::vector<int64_t> still;
@@ -561,7 +628,7 @@ static int server_step(Server &S) {
     Job &J = S.jobs[id];
     auto it = got.find(id);
     if (it != got.end()) J.spp_done += it->second;
-    if (J.spp_done >= J.req.spp) {
+    if (J.spp_done >= J.req.spp || J.converged) {
       J.state = 2;
       J.t_done = t;
       S.stats.jobs_done++;
@@ -596,6 +663,8 @@ void rb_job_default(rb_job_request *r) {
   r->glass_ior = 1.5f;
   r->dof_aperture = 0.1f;
   r->dof_focus = 10.0f;
+  r->converge_min_spp = 32;    // the reference's min_adaptive_samples default
+  r->converge_fraction = 1.0f;
 }
 
 void rb_server_default_opts(rb_server_opts *o) {
@@ -632,7 +701,9 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   bool ok = cuda_ok(cudaMallocHost(&S.h_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server pinned jobs") &&
             cuda_ok(cudaMalloc(&S.d_jobs, sizeof(BatchJob) * S.o.max_active_jobs), "server jobs") &&
             cuda_ok(cudaMallocHost(&S.h_ctl, sizeof(BatchCtl) * RB_GROUPS), "server pinned ctl") &&
-            cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * RB_GROUPS), "server ctl");
+            cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * RB_GROUPS), "server ctl") &&
+            cuda_ok(cudaMallocHost(&S.h_conv, sizeof(unsigned long long) * S.o.max_active_jobs), "server conv") &&
+            cuda_ok(cudaMalloc(&S.d_conv, sizeof(unsigned long long) * S.o.max_active_jobs), "server conv");
   if (!ok) {
     rb_server_destroy(r);
     return nullptr;
@@ -658,6 +729,8 @@ void rb_server_destroy(rb_server *r) {
   if (S.d_jobs) cudaFree(S.d_jobs);
   if (S.h_ctl) cudaFreeHost(S.h_ctl);
   if (S.d_ctl) cudaFree(S.d_ctl);
+  if (S.h_conv) cudaFreeHost(S.h_conv);
+  if (S.d_conv) cudaFree(S.d_conv);
   if (S.ev0) cudaEventDestroy(S.ev0);
   if (S.ev1) cudaEventDestroy(S.ev1);
   if (S.own_stream && S.st) cudaStreamDestroy(S.st);
@@ -679,7 +752,8 @@ int64_t rb_server_submit(rb_server *r, const rb_job_request *q) {
   if (!r || !q) return RB_ERR_INVALID_ARG;
   Server &S = r->s;
   if (q->scene < 0 || q->scene >= (int)S.scenes.size() || q->width <= 0 || q->height <= 0 || q->spp <= 0 ||
-      q->max_depth < 0 || (int64_t)q->width * q->height > (1ll << 31) - 1) {
+      q->max_depth < 0 || (int64_t)q->width * q->height > (1ll << 31) - 1 ||
+      (q->converge_threshold > 0.0f && !(q->converge_fraction > 0.0f && q->converge_fraction <= 1.0f))) {
     set_error("rb_server_submit: invalid request");
     return RB_ERR_INVALID_ARG;
   }

@@ -11,7 +11,9 @@ from ._native import JobRequest, JobStatus, ServerOpts, ServerStats, check, lib
 
 def job(scene: int, frame, width: int, height: int, spp: int, depth: int, background: float = 1.0,
         dof: tuple | None = None, nee: bool = False, seed: int = 0, fp64: bool = False, arrival: float = 0.0,
-        light: float = 1.0, fuzz: float = 0.8, glass_ior: float = 1.5) -> JobRequest:
+        light: float = 1.0, fuzz: float = 0.8, glass_ior: float = 1.5, converge: tuple | None = None) -> JobRequest:
+    """converge = (threshold, min_spp, fraction): complete the job early once
+    that fraction of its pixels change by less than the threshold per iteration."""
     r = JobRequest()
     lib.rb_job_default(C.byref(r))
     r.scene, r.width, r.height, r.spp, r.max_depth = scene, width, height, spp, depth
@@ -20,6 +22,9 @@ def job(scene: int, frame, width: int, height: int, spp: int, depth: int, backgr
     if dof is not None:
         r.dof_enabled, r.dof_aperture, r.dof_focus = 1, float(dof[0]), float(dof[1])
     r.nee, r.seed, r.fp64_accum, r.arrival_time = int(nee), int(seed), int(fp64), float(arrival)
+    if converge is not None:
+        r.converge_threshold, r.converge_min_spp, r.converge_fraction = (float(converge[0]), int(converge[1]),
+                                                                         float(converge[2]))
     return r
 
 

@@ -200,3 +200,27 @@ def test_latency_target_controller(cuda):
     assert tail and 0.4 * target < float(np.median(tail)) < 2.5 * target, ms
     srv.close()
     ds.free()
+
+
+def test_per_job_convergence(cuda):
+    # a job with a convergence test completes before its spp once its pixels
+    # stop changing; its image agrees with the full-spp render (per sample)
+    spec = scenes.cornell(width=48, height=48)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = spec.camera.frame(48, 48)
+    srv = serving.Server(paths_per_iteration=48 * 48 * 64, max_spp_per_iteration=64)
+    sid = srv.add_scene(ds)
+    early = srv.submit(serving.job(sid, fr, 48, 48, 16384, spec.depth, background=0.0, seed=1,
+                                   converge=(0.01, 128, 0.95)))
+    full = srv.submit(serving.job(sid, fr, 48, 48, 4096, spec.depth, background=0.0, seed=2))
+    srv.drain()
+    se, sf = srv.status(early), srv.status(full)
+    assert se.state == 2 and sf.state == 2
+    assert 128 <= se.spp_done < 16384 and sf.spp_done == 4096
+    a = srv.fetch(early, 48, 48) / se.spp_done
+    b = srv.fetch(full, 48, 48) / sf.spp_done
+    np.testing.assert_allclose(a.mean(), b.mean(), rtol=0.05)
+    srv.close()
+    ds.free()
