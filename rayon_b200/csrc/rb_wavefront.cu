@@ -174,40 +174,47 @@ __global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi
 // WF_CAND_REG candidate records are passed in registers (loaded once per ray),
 // the rest are read from the slot's records.
 #define WF_CAND_REG 4
-struct WfFold {
-  float F = RB_SDF_FAR, best = RB_SDF_FAR, next = RB_SDF_FAR;
-  bool first = true;
-  // tab: the SDF table staged in shared memory (5 words per record), or null
-  __device__ __forceinline__ void add(const SceneView &S, const float4 *tab, const int4 e, const f3 &p, float t,
-                                      int *nearest) {
+__device__ __forceinline__ int4 wf_cand(const WfParams &W, const int4 (&cr)[WF_CAND_REG], int slot, int i) {
+  int4 e = cr[0];
+#pragma unroll
+  for (int k = 1; k < WF_CAND_REG; ++k)
+    if (i == k) e = cr[k];
+  return i < WF_CAND_REG ? e : __ldg(W.cand + (size_t)i * W.cap + slot);
+}
+
+// Two passes so that a warp's lanes evaluate together: first each lane marks,
+// in index order, its candidates whose window holds t (and the next window
+// entry beyond t); then the lanes fold their k-th marked candidate at the
+// same time, k = 0, 1, ... (the fold order per lane is still index order).
+__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, const float4 *tab, int slot, int n,
+                                          const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
+                                          int *nearest) {
+  uint32_t active = 0;
+  float nx = RB_SDF_FAR;
+  for (int i = 0; i < n; ++i) {
+    const int4 e = wf_cand(W, cr, slot, i);
     const float t0 = __int_as_float(e.y);
-    if (t0 > t) {
-      next = fminf(next, t0);
-      return;
-    }
-    if (t > __int_as_float(e.z)) return;
-    const float d = tab ? sdf_eval_words(tab[5 * e.x], tab[5 * e.x + 1], tab[5 * e.x + 2], tab[5 * e.x + 3],
-                                         tab[5 * e.x + 4], p)
-                        : sdf_eval_at(S.sdf, e.x, p);
+    if (t0 > t) nx = fminf(nx, t0);
+    else if (t <= __int_as_float(e.z)) active |= 1u << i;
+  }
+  next = nx;
+  float F = RB_SDF_FAR, best = RB_SDF_FAR;
+  bool first = true;
+  while (active) {
+    const int i = __ffs(active) - 1;
+    active &= active - 1;
+    const int id = wf_cand(W, cr, slot, i).x;
+    const float d = tab ? sdf_eval_words(tab[5 * id], tab[5 * id + 1], tab[5 * id + 2], tab[5 * id + 3],
+                                         tab[5 * id + 4], p)
+                        : sdf_eval_at(S.sdf, id, p);
     if (nearest && d < best) {
       best = d;
-      *nearest = e.x;
+      *nearest = id;
     }
     F = first ? d : smin_poly(F, d, S.sdf_k);
     first = false;
   }
-};
-
-__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, const float4 *tab, int slot, int n,
-                                          const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
-                                          int *nearest) {
-  WfFold f;
-#pragma unroll
-  for (int i = 0; i < WF_CAND_REG; ++i)
-    if (i < n) f.add(S, tab, cr[i], p, t, nearest);
-  for (int i = WF_CAND_REG; i < n; ++i) f.add(S, tab, __ldg(W.cand + (size_t)i * W.cap + slot), p, t, nearest);
-  next = f.next;
-  return f.F;
+  return F;
 }
 
 // Persistent field march over the march list. Every pass, each busy lane
