@@ -22,6 +22,11 @@ inline float __uint_as_float_host(uint32_t i) {
   std::memcpy(&f, &i, 4);
   return f;
 }
+inline uint32_t __float_as_uint_host(float f) {
+  uint32_t i;
+  std::memcpy(&i, &f, 4);
+  return i;
+}
 
 // Device layout assembled on the host before upload.
 struct HostLayout {

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -122,6 +123,23 @@ static void rot_matrix(const double r[3], float out[9]) {
     for (int j = 0; j < 3; ++j) out[3 * i + j] = (float)R[j][i];
 }
 
+// Runs fn(begin, end) over [0, n) in contiguous chunks on the host's cores.
+template <class F>
+static void parallel_chunks(size_t n, F fn) {
+  const size_t threads = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 64);
+  if (n < 65536 || threads == 1) {
+    fn((size_t)0, n);
+    return;
+  }
+  const size_t chunk = (n + threads - 1) / threads;
+  std::vector<std::thread> pool;
+  for (size_t t = 0; t < threads; ++t) {
+    const size_t b = t * chunk, e = std::min(n, b + chunk);
+    if (b < e) pool.emplace_back(fn, b, e);
+  }
+  for (auto &th : pool) th.join();
+}
+
 static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts, HostLayout &L) {
   const size_t n = hs.geoms.size();
   L.prims.assign(3 * n, make_float4(0, 0, 0, 0));
@@ -132,73 +150,87 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
   if (any_normals) L.normals.assign(3 * n, make_float4(0, 0, 0, 0));
   L.sdf.clear();
   double light_area = 0.0;
+  auto tag_of = [&](const Geom &g, uint32_t kind) {
+    const uint32_t mat =
+        (g.material_id >= 0 && g.material_id < (int)hs.materials.size()) ? (uint32_t)g.material_id : 0xFFFFFFu;
+    return kind | ((uint32_t)(g.visible ? 1 : 0) << 3) | ((uint32_t)((g.has_normals && any_normals) ? 1 : 0) << 4) |
+           (mat << 8);
+  };
+  // records of spheres, quads and triangles, in parallel (each writes its own
+  // slots); SDF primitives and emitters follow in order below
+  parallel_chunks(n, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      const Geom &g = hs.geoms[i];
+      float4 *r = &L.prims[3 * i];
+      uint32_t kind = PK_NONE;
+      switch (g.type) {
+        case RB_GEOM_SPHERE:
+        case RB_GEOM_DISPLACED_SPHERE:
+          kind = g.type == RB_GEOM_SPHERE ? PK_SPHERE : PK_DISPLACED;
+          for (int k = 0; k < 4; ++k) put(r, k, (float)g.p[k]);
+          break;
+        case RB_GEOM_RECTANGLE:
+          kind = PK_RECT;
+          for (int k = 0; k < 9; ++k) put(r, k, (float)g.p[k]);
+          break;
+        case RB_GEOM_TRIANGLE: {
+          kind = PK_TRI;
+          float v[9];
+          for (int k = 0; k < 9; ++k) v[k] = (float)g.p[k];
+          for (int k = 0; k < 3; ++k) {
+            put(r, k, v[k]);
+            put(r, 3 + k, ftz_sub(v[3 + k], v[k]));
+            put(r, 6 + k, ftz_sub(v[6 + k], v[k]));
+          }
+          if (g.has_normals && any_normals)
+            for (int k = 0; k < 3; ++k)
+              L.normals[3 * i + k] =
+                  make_float4((float)g.p[9 + 3 * k], (float)g.p[10 + 3 * k], (float)g.p[11 + 3 * k], 0.0f);
+          break;
+        }
+        case RB_GEOM_SDF_PRIMITIVE:
+          continue;  // below, in order (the SDF table index)
+        default:
+          kind = PK_NONE;  // CUBE / TRIANGLE_MESH are not converted (scene_builder_cuda.cu:138-140)
+          break;
+      }
+      put(r, 11, __uint_as_float_host(tag_of(g, kind)));
+    }
+  });
   for (size_t i = 0; i < n; ++i) {
     const Geom &g = hs.geoms[i];
     float4 *r = &L.prims[3 * i];
-    uint32_t kind = PK_NONE;
-    const float *pf = nullptr;
-    (void)pf;
-    switch (g.type) {
-      case RB_GEOM_SPHERE:
-      case RB_GEOM_DISPLACED_SPHERE:
-        kind = g.type == RB_GEOM_SPHERE ? PK_SPHERE : PK_DISPLACED;
-        for (int k = 0; k < 4; ++k) put(r, k, (float)g.p[k]);
-        break;
-      case RB_GEOM_RECTANGLE:
-        kind = PK_RECT;
-        for (int k = 0; k < 9; ++k) put(r, k, (float)g.p[k]);
-        break;
-      case RB_GEOM_TRIANGLE: {
-        kind = PK_TRI;
-        float v[9];
-        for (int k = 0; k < 9; ++k) v[k] = (float)g.p[k];
-        for (int k = 0; k < 3; ++k) {
-          put(r, k, v[k]);
-          put(r, 3 + k, ftz_sub(v[3 + k], v[k]));
-          put(r, 6 + k, ftz_sub(v[6 + k], v[k]));
-        }
-        if (g.has_normals && any_normals)
-          for (int k = 0; k < 3; ++k)
-            L.normals[3 * i + k] = make_float4((float)g.p[9 + 3 * k], (float)g.p[10 + 3 * k], (float)g.p[11 + 3 * k], 0.0f);
-        break;
+    uint32_t kind = tag_kind(__float_as_uint_host(getw(r, 11)));
+    if (g.type == RB_GEOM_SDF_PRIMITIVE) {
+      kind = PK_SDF;
+      SdfPrim q;
+      std::memset(&q, 0, sizeof q);
+      const int t = (int)g.p[0];
+      q.type = (t == RB_SDF_ROUND_BOX) ? 32 : t;
+      q.material = g.material_id;
+      q.px = (float)g.p[1]; q.py = (float)g.p[2]; q.pz = (float)g.p[3];
+      q.a = (float)g.p[4]; q.b = (float)g.p[5]; q.c = (float)g.p[6];
+      if (t != RB_SDF_SPHERE && t != RB_SDF_BOX && t != RB_SDF_ROUND_BOX && t != RB_SDF_TORUS &&
+          t != RB_SDF_CAPSULE) {
+        put(r, 11, __uint_as_float_host(tag_of(g, PK_NONE)));
+        continue;
       }
-      case RB_GEOM_SDF_PRIMITIVE: {
-        kind = PK_SDF;
-        SdfPrim q;
-        std::memset(&q, 0, sizeof q);
-        const int t = (int)g.p[0];
-        q.type = (t == RB_SDF_ROUND_BOX) ? 32 : t;
-        q.material = g.material_id;
-        q.px = (float)g.p[1]; q.py = (float)g.p[2]; q.pz = (float)g.p[3];
-        q.a = (float)g.p[4]; q.b = (float)g.p[5]; q.c = (float)g.p[6];
-        if (t != RB_SDF_SPHERE && t != RB_SDF_BOX && t != RB_SDF_ROUND_BOX && t != RB_SDF_TORUS &&
-            t != RB_SDF_CAPSULE) {
-          kind = PK_NONE;
-          break;
-        }
-        const double bound = sdf_bound_radius(g);
-        // rounded box: half extents in params, rounding radius = 0.2 x the smallest half extent
-        if (t == RB_SDF_ROUND_BOX) q.round = (float)(0.2 * std::min(g.p[4], std::min(g.p[5], g.p[6])));
-        float R[9];
-        const double rr[3] = {g.p[7], g.p[8], g.p[9]};
-        rot_matrix(rr, R);
-        q.r00 = R[0]; q.r01 = R[1]; q.r02 = R[2]; q.r10 = R[3]; q.r11 = R[4]; q.r12 = R[5];
-        q.r20 = R[6]; q.r21 = R[7]; q.r22 = R[8];
-        const double pad = hs.sdf.blend_k + 1e-3;
-        put(r, 0, q.px); put(r, 1, q.py); put(r, 2, q.pz); put(r, 3, (float)(bound * 1.0001 + pad));
-        put(r, 4, __int_as_float_host((int)L.sdf.size()));
-        L.sdf.push_back(q);
-        break;
-      }
-      default:
-        kind = PK_NONE;  // CUBE / TRIANGLE_MESH are not converted (scene_builder_cuda.cu:138-140)
-        break;
+      const double bound = sdf_bound_radius(g);
+      // rounded box: half extents in params, rounding radius = 0.2 x the smallest half extent
+      if (t == RB_SDF_ROUND_BOX) q.round = (float)(0.2 * std::min(g.p[4], std::min(g.p[5], g.p[6])));
+      float R[9];
+      const double rr[3] = {g.p[7], g.p[8], g.p[9]};
+      rot_matrix(rr, R);
+      q.r00 = R[0]; q.r01 = R[1]; q.r02 = R[2]; q.r10 = R[3]; q.r11 = R[4]; q.r12 = R[5];
+      q.r20 = R[6]; q.r21 = R[7]; q.r22 = R[8];
+      const double pad = hs.sdf.blend_k + 1e-3;
+      put(r, 0, q.px); put(r, 1, q.py); put(r, 2, q.pz); put(r, 3, (float)(bound * 1.0001 + pad));
+      put(r, 4, __int_as_float_host((int)L.sdf.size()));
+      L.sdf.push_back(q);
+      put(r, 11, __uint_as_float_host(tag_of(g, kind)));
     }
-    uint32_t mat = (g.material_id >= 0 && g.material_id < (int)hs.materials.size()) ? (uint32_t)g.material_id : 0xFFFFFFu;
-    const uint32_t tag = kind | ((uint32_t)(g.visible ? 1 : 0) << 3) |
-                         ((uint32_t)((g.has_normals && any_normals) ? 1 : 0) << 4) | (mat << 8);
-    put(r, 11, __uint_as_float_host(tag));
     // emitters for next-event estimation
+    const uint32_t mat = (uint32_t)tag_material(__float_as_uint_host(getw(r, 11))) & 0xFFFFFFu;
     if (mat != 0xFFFFFFu && L.mats[mat].kind == L_LIGHT &&
         (kind == PK_RECT || kind == PK_TRI || kind == PK_SPHERE)) {
       const DevMaterial &m = L.mats[mat];
@@ -251,24 +283,29 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
       if (c.is_leaf) return make_leaf_ref(c.a, std::max(1, c.b));
       return remap[i];
     };
-    for (size_t i = 0; i < hs.nodes.size(); ++i) {
-      const Node &nd = hs.nodes[i];
-      if (nd.is_leaf) {
-        if (nd.a >= (1 << 26) || nd.b > 32) { set_error("BVH leaf beyond the device encoding"); return false; }
-        continue;
+    for (const Node &nd : hs.nodes)
+      if (nd.is_leaf && (nd.a >= (1 << 26) || nd.b > 32)) {
+        set_error("BVH leaf beyond the device encoding");
+        return false;
       }
-      const Node &l = hs.nodes[nd.a], &rr = hs.nodes[nd.b];
-      float4 q[4];
-      float *w = reinterpret_cast<float *>(q);
-      for (int k = 0; k < 3; ++k) { w[k] = (float)l.bmin[k]; w[3 + k] = (float)l.bmax[k]; }
-      for (int k = 0; k < 3; ++k) { w[6 + k] = (float)rr.bmin[k]; w[9 + k] = (float)rr.bmax[k]; }
-      int *wi = reinterpret_cast<int *>(&q[3]);
-      wi[0] = ref_of(nd.a);
-      wi[1] = ref_of(nd.b);
-      wi[2] = nd.split_axis;
-      wi[3] = 0;
-      for (int k = 0; k < 4; ++k) L.nodes.push_back(q[k]);
-    }
+    // interior node i goes to slot remap[i]: independent writes, in parallel
+    L.nodes.assign(4 * (size_t)m, make_float4(0, 0, 0, 0));
+    parallel_chunks(hs.nodes.size(), [&](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) {
+        const Node &nd = hs.nodes[i];
+        if (nd.is_leaf) continue;
+        const Node &l = hs.nodes[nd.a], &rr = hs.nodes[nd.b];
+        float4 *q = &L.nodes[4 * (size_t)remap[i]];
+        float *w = reinterpret_cast<float *>(q);
+        for (int k = 0; k < 3; ++k) { w[k] = (float)l.bmin[k]; w[3 + k] = (float)l.bmax[k]; }
+        for (int k = 0; k < 3; ++k) { w[6 + k] = (float)rr.bmin[k]; w[9 + k] = (float)rr.bmax[k]; }
+        int *wi = reinterpret_cast<int *>(&q[3]);
+        wi[0] = ref_of(nd.a);
+        wi[1] = ref_of(nd.b);
+        wi[2] = nd.split_axis;
+        wi[3] = 0;
+      }
+    });
     const Node &root = hs.nodes[hs.root];
     for (int k = 0; k < 3; ++k) { L.root_box[k] = (float)root.bmin[k]; L.root_box[3 + k] = (float)root.bmax[k]; }
     L.root_ref = ref_of(hs.root);
