@@ -233,13 +233,20 @@ typedef struct rb_upload_opts {
  * from rb_scene_build_bvh: primary-hit ids bit-exact against the reference).
  * RB_LAYOUT_AUTOTUNE: time a probe render (256 x 256 samples of probe_frame's
  * view, 8 spp; without a frame, views from inside and outside the scene's box)
- * on each candidate layout (linear scan for small scenes, BVH leaf sizes
- * 1/2/4/8) and keep the fastest; decisions are cached per scene.
- * RB_LAYOUT_LINEAR: no BVH. RB_LAYOUT_LEAF: rebuild the BVH with max_leaf. */
-enum { RB_LAYOUT_AS_BUILT = 0, RB_LAYOUT_AUTOTUNE = 1, RB_LAYOUT_LINEAR = 2, RB_LAYOUT_LEAF = 3 };
+ * on each candidate layout (linear scan and groups of 8 / 16 for small
+ * scenes, BVH leaf sizes 1/2/4/8) and keep the fastest; decisions are cached
+ * per scene.
+ * RB_LAYOUT_LINEAR: no BVH. RB_LAYOUT_LEAF: rebuild the BVH with max_leaf.
+ * RB_LAYOUT_GROUPS: no traversal stack: the built BVH's largest subtrees of at
+ * most max_leaf primitives become groups, tested in leaf order (the group's
+ * box, then its primitives); the primitives are tested in the linear scan's
+ * order. */
+enum { RB_LAYOUT_AS_BUILT = 0, RB_LAYOUT_AUTOTUNE = 1, RB_LAYOUT_LINEAR = 2, RB_LAYOUT_LEAF = 3,
+       RB_LAYOUT_GROUPS = 4 };
 
-/* Layout the upload chose: kind (RB_LAYOUT_LINEAR or RB_LAYOUT_LEAF),
- * leaf size (0 for linear) and, when autotuned, the probe time of the winner. */
+/* Layout the upload chose: kind (RB_LAYOUT_LINEAR, RB_LAYOUT_LEAF or
+ * RB_LAYOUT_GROUPS), leaf or group size (0 for linear) and, when autotuned,
+ * the probe time of the winner. */
 int rb_scene_layout_info(const rb_cuda_scene *scene, int *kind, int *leaf, float *probe_ms);
 
 /* Upload to the current device. Returns an opaque device-scene handle that is

@@ -145,6 +145,8 @@ struct SceneView {
   const DevMaterial *__restrict__ mats;
   const LightRec *__restrict__ lights;
   const SdfPrim *__restrict__ sdf;
+  const float4 *__restrict__ groups;  // 2 per group: (box min, first primitive), (box max, count)
+  int num_groups;                     // > 0: grouped linear layout (no BVH traversal)
   int root_ref;
   int num_prims;
   int num_mats;
@@ -266,6 +268,7 @@ static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &
 // each with the ray interval [t0, t1] inside its sphere, and the union field
 // of those is sphere-traced after the traversal.
 #define RB_SDF_CAND 24
+static_assert(RB_SDF_CAND <= 32, "field folds mark candidates in a 32-bit mask");
 struct SdfCand {
   int n;
   int idx[RB_SDF_CAND];
@@ -408,6 +411,28 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
   h.t = tmax;
   h.prim = -1;
   float closest = tmax;
+  if (S.num_groups > 0) {
+    // grouped linear layout: groups in leaf order; a group's primitives are
+    // tested (in index order, as by the linear scan) when its box is entered
+    // before the closest hit
+    const RayPre rp = prep(ray);
+    for (int gi = 0; gi < S.num_groups; ++gi) {
+      const float4 g0 = __ldg(S.groups + 2 * gi), g1 = __ldg(S.groups + 2 * gi + 1);
+      float te;
+      if (!box_hit(rp, g0.x, g0.y, g0.z, g1.x, g1.y, g1.z, tmin, closest, te)) continue;
+      const int first = __float_as_int(g0.w), end = first + __float_as_int(g1.w);
+      for (int i = first; i < end; ++i) {
+        float t;
+        if (prim_t<MS>(S, i, ray, tmin, closest, t, cand)) {
+          closest = t;
+          h.t = t;
+          h.prim = i;
+          if (ANY) return h;
+        }
+      }
+    }
+    return h;
+  }
   if (!S.use_bvh) {
     for (int i = 0; i < S.num_prims; ++i) {
       float t;

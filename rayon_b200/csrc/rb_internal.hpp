@@ -37,6 +37,7 @@ struct HostLayout {
   std::vector<rbd::DevMaterial> mats;
   std::vector<rbd::LightRec> lights;
   std::vector<rbd::SdfPrim> sdf;
+  std::vector<float4> groups;         // grouped linear layout: 2 per group
   int root_ref = 0;
   float root_box[6] = {0, 0, 0, 0, 0, 0};
   float light_area = 0.0f;

@@ -314,6 +314,48 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
       L.nodes.clear();  // the quantised copy replaces the FP32 nodes on the device
     }
   }
+  L.groups.clear();
+  if (opts.layout == RB_LAYOUT_GROUPS && hs.use_bvh && !hs.nodes.empty() && hs.root >= 0) {
+    // the largest subtrees of at most G primitives, in leaf order; a subtree's
+    // primitives are contiguous because the geometries are in the tree's leaf order
+    const int G = std::max(1, opts.max_leaf);
+    std::vector<int> first(hs.nodes.size()), count(hs.nodes.size());
+    std::vector<std::pair<int, bool>> todo{{hs.root, false}};
+    while (!todo.empty()) {  // post-order ranges
+      const auto [ni, done] = todo.back();
+      todo.pop_back();
+      const Node &nd = hs.nodes[ni];
+      if (nd.is_leaf) {
+        first[ni] = nd.a;
+        count[ni] = std::max(1, nd.b);
+      } else if (done) {
+        first[ni] = first[nd.a];
+        count[ni] = count[nd.a] + count[nd.b];
+      } else {
+        todo.push_back({ni, true});
+        todo.push_back({nd.b, false});
+        todo.push_back({nd.a, false});
+      }
+    }
+    std::vector<int> stack{hs.root};
+    while (!stack.empty()) {  // pre-order, left child first: leaf order
+      const int ni = stack.back();
+      stack.pop_back();
+      const Node &nd = hs.nodes[ni];
+      if (nd.is_leaf || count[ni] <= G) {
+        L.groups.push_back(make_float4((float)nd.bmin[0], (float)nd.bmin[1], (float)nd.bmin[2],
+                                       __int_as_float_host(first[ni])));
+        L.groups.push_back(make_float4((float)nd.bmax[0], (float)nd.bmax[1], (float)nd.bmax[2],
+                                       __int_as_float_host(count[ni])));
+      } else {
+        stack.push_back(nd.b);
+        stack.push_back(nd.a);
+      }
+    }
+    L.use_bvh = false;
+    L.nodes.clear();
+    L.qnodes.clear();
+  }
   return true;
 }
 
@@ -336,6 +378,7 @@ void free_device_scene(DeviceScene *ds) {
   cudaFree((void *)ds->view.mats);
   cudaFree((void *)ds->view.lights);
   cudaFree((void *)ds->view.sdf);
+  cudaFree((void *)ds->view.groups);
   cudaFree(ds->handle);
   delete ds;
 }
@@ -352,12 +395,14 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
   DevMaterial *mats = nullptr;
   LightRec *lights = nullptr;
   SdfPrim *sdf = nullptr;
+  float4 *groups = nullptr;
   bool ok = upload_vec(L.nodes, &nodes, st, bytes) && upload_vec(L.qnodes, &qn, st, bytes) &&
             upload_vec(L.prims, &prims, st, bytes) && upload_vec(L.normals, &normals, st, bytes) &&
             upload_vec(L.mats, &mats, st, bytes) && upload_vec(L.lights, &lights, st, bytes) &&
-            upload_vec(L.sdf, &sdf, st, bytes);
+            upload_vec(L.sdf, &sdf, st, bytes) && upload_vec(L.groups, &groups, st, bytes);
   v.nodes = nodes; v.qnodes = qn; v.prims = prims; v.normals = normals; v.mats = mats;
-  v.lights = lights; v.sdf = sdf;
+  v.lights = lights; v.sdf = sdf; v.groups = groups;
+  v.num_groups = (int)(L.groups.size() / 2);
   v.root_ref = L.root_ref;
   v.num_prims = (int)hs.geoms.size();
   v.num_mats = (int)hs.materials.size();
@@ -377,8 +422,8 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
        cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize(upload)");
   ds->bytes = bytes + 256;
   ds->ms = L.ms;
-  ds->layout_kind = L.use_bvh ? RB_LAYOUT_LEAF : RB_LAYOUT_LINEAR;
-  ds->layout_leaf = L.use_bvh ? hs.max_leaf : 0;
+  ds->layout_kind = !L.groups.empty() ? RB_LAYOUT_GROUPS : L.use_bvh ? RB_LAYOUT_LEAF : RB_LAYOUT_LINEAR;
+  ds->layout_leaf = !L.groups.empty() ? std::max(1, opts.max_leaf) : L.use_bvh ? hs.max_leaf : 0;
   if (!ok) {
     free_device_scene(ds);
     return nullptr;
@@ -811,7 +856,12 @@ struct TuneKey {
 struct TuneKeyHash {
   size_t operator()(const TuneKey &k) const { return (size_t)(k.fp ^ ((uint64_t)k.dev << 56)); }
 };
-static std::unordered_map<TuneKey, std::pair<bool, int>, TuneKeyHash> g_tune_cache;
+struct TuneChoice {
+  bool linear;
+  int leaf;    // BVH leaf size
+  int groups;  // > 0: grouped linear layout with groups of at most this many primitives
+};
+static std::unordered_map<TuneKey, TuneChoice, TuneKeyHash> g_tune_cache;
 
 static uint64_t scene_fingerprint(const HostScene &hs) {
   uint64_t h = 1469598103934665603ull;
@@ -831,7 +881,7 @@ static uint64_t scene_fingerprint(const HostScene &hs) {
 DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cudaStream_t st) {
   const int depth = o0.tune_depth > 0 ? o0.tune_depth : 8;
   const std::vector<FrameF> frames = probe_frames(hs, o0, depth);
-  struct Cand { bool linear; int leaf; };
+  using Cand = TuneChoice;
   std::vector<Cand> cands;
   const size_t n = hs.geoms.size();
   int dev = 0;
@@ -842,15 +892,19 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      cands.push_back({it->second.first, it->second.second});
+      cands.push_back(it->second);
       cached = true;
     }
   }
   if (!cached) {
-    if (n <= 4096) cands.push_back({true, 0});
+    if (n <= 4096) {
+      cands.push_back({true, 0, 0});
+      if (hs.use_bvh && !hs.nodes.empty())
+        for (int G : {8, 16}) cands.push_back({false, 0, G});
+    }
     if (n > 0) {
-      if (n > (1u << 20)) cands.push_back({false, 1}), cands.push_back({false, 4});
-      else for (int L : {1, 2, 4, 8}) cands.push_back({false, L});
+      if (n > (1u << 20)) cands.push_back({false, 1, 0}), cands.push_back({false, 4, 0});
+      else for (int L : {1, 2, 4, 8}) cands.push_back({false, L, 0});
     }
   }
   DeviceScene *best = nullptr;
@@ -862,6 +916,11 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
     if (c.linear) {
       o.use_bvh = 0;
       ds = upload_scene(hs, o, st);
+    } else if (c.groups > 0) {
+      o.use_bvh = 1;
+      o.layout = RB_LAYOUT_GROUPS;
+      o.max_leaf = c.groups;
+      ds = upload_scene(hs, o, st);
     } else if (hs.use_bvh && hs.max_leaf == c.leaf && !hs.nodes.empty()) {
       o.use_bvh = 1;
       ds = upload_scene(hs, o, st);
@@ -872,8 +931,8 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
       ds = upload_scene(copy, o, st);
     }
     if (!ds) continue;
-    ds->layout_kind = c.linear ? RB_LAYOUT_LINEAR : RB_LAYOUT_LEAF;
-    ds->layout_leaf = c.leaf;
+    ds->layout_kind = c.linear ? RB_LAYOUT_LINEAR : c.groups > 0 ? RB_LAYOUT_GROUPS : RB_LAYOUT_LEAF;
+    ds->layout_leaf = c.groups > 0 ? c.groups : c.leaf;
     if (cands.size() == 1) {  // cached (or only) choice: no probing
       best = ds;
       break;
@@ -894,7 +953,9 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
   }
   if (!cached) {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_tune_cache[key] = {best->layout_kind == RB_LAYOUT_LINEAR, best->layout_leaf};
+    const bool groups = best->layout_kind == RB_LAYOUT_GROUPS;
+    g_tune_cache[key] = {best->layout_kind == RB_LAYOUT_LINEAR, groups ? 0 : best->layout_leaf,
+                         groups ? best->layout_leaf : 0};
   }
   return best;
 }

@@ -521,16 +521,20 @@ __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
 // holds t.
 __device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCand &c, const f3 &p, float t,
                                                 float &next, int *nearest) {
-  float F = RB_SDF_FAR, best = RB_SDF_FAR;
-  bool first = true;
+  // two passes so that a warp's lanes evaluate together: mark the candidates
+  // whose window holds t (index order), then fold the marked ones
+  uint32_t active = 0;
   next = RB_SDF_FAR;
   for (int i = 0; i < c.n; ++i) {
     const float t0 = c.t0[i];
-    if (t0 > t) {
-      next = fminf(next, t0);
-      continue;
-    }
-    if (t > c.t1[i]) continue;
+    if (t0 > t) next = fminf(next, t0);
+    else if (t <= c.t1[i]) active |= 1u << i;
+  }
+  float F = RB_SDF_FAR, best = RB_SDF_FAR;
+  bool first = true;
+  while (active) {
+    const int i = __ffs(active) - 1;
+    active &= active - 1;
     const float d = sdf_eval_at(S.sdf, c.idx[i], p);
     if (nearest && d < best) {
       best = d;

@@ -223,11 +223,13 @@ class SceneDescription:
     def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None, layout: str = "as_built",
                max_leaf: int = 0, tune_depth: int = 0, probe=None) -> "DeviceScene":
         """layout: "as_built" (the built BVH; bit-exact primary hits), "autotune"
-        (fastest of linear / leaf 1, 2, 4, 8 on a probe render), "linear", "leaf"."""
+        (fastest of linear / groups of 8, 16 / leaf 1, 2, 4, 8 on a probe render),
+        "linear", "leaf" (rebuilt with max_leaf), "groups" (the built BVH's subtrees of
+        at most max_leaf primitives tested in order, no traversal stack)."""
         o = UploadOpts()
         o.quantized_bvh = int(quantized)
         o.use_bvh = int(use_bvh)
-        o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3}[layout]
+        o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3, "groups": 4}[layout]
         o.max_leaf = int(max_leaf)
         o.tune_depth = int(tune_depth)
         keep = None
@@ -255,7 +257,8 @@ class DeviceScene:
     def layout(self) -> dict:
         k, leaf, ms = C.c_int32(0), C.c_int32(0), C.c_float(0)
         lib.rb_scene_layout_info(self.handle, C.byref(k), C.byref(leaf), C.byref(ms))
-        return {"kind": "linear" if k.value == 2 else "bvh", "leaf": leaf.value, "probe_ms": ms.value}
+        kind = {2: "linear", 4: "groups"}.get(k.value, "bvh")
+        return {"kind": kind, "leaf": leaf.value, "probe_ms": ms.value}
 
     def free(self) -> None:
         if self.handle:

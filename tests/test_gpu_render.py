@@ -166,7 +166,7 @@ def test_autotuned_layout_renders_the_same(cuda, name):
     a_ds = sc.upload()
     t_ds = sc.upload(layout="autotune", tune_depth=spec.depth)
     info = t_ds.layout
-    assert info["kind"] in ("linear", "bvh") and info["probe_ms"] > 0
+    assert info["kind"] in ("linear", "groups", "bvh") and info["probe_ms"] > 0
     a = render.render_accumulate(a_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
     b = render.render_accumulate(t_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
     # same sample streams; layouts can only differ on exact-t ties
@@ -197,3 +197,24 @@ def test_wavefront_engine_paired_with_per_pixel_kernel(cuda, name, nee):
     assert bad.mean() < 0.01, bad.mean()
     np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=1e-2, atol=1e-4)
     ds.free()
+
+
+@pytest.mark.parametrize("name", ["cornell", "one_weekend"])
+def test_grouped_layout_renders_the_same(cuda, name):
+    # groups of the built tree's subtrees, primitives tested in the linear
+    # scan's order: the same closest hits as the linear scan, so the same paths
+    spec, _ = _cases()[name]
+    w, h, spp = 48, 32, 8
+    sc = spec.to_scene()
+    sc.build_bvh()
+    lin = sc.upload(layout="linear")
+    fr = spec.camera.frame(w, h)
+    a = render.render_accumulate(lin, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
+    for g in (1, 8, 16):
+        grp = sc.upload(layout="groups", max_leaf=g)
+        assert grp.layout["kind"] == "groups" and grp.layout["leaf"] == g
+        b = render.render_accumulate(grp, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof)
+        bad = (np.abs(a - b) > 1e-3 * (1 + np.abs(a)) * spp).any(axis=2)
+        assert bad.mean() < 0.005, (g, bad.mean())
+        grp.free()
+    lin.free()
