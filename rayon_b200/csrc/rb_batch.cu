@@ -207,8 +207,19 @@ static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob 
   switch (minb) {
     case 1: k_batch<MS, 1, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
     case 3: k_batch<MS, 3, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 4: k_batch<MS, 4, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
     default: k_batch<MS, 2, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
   }
+}
+
+// Resident 256-thread blocks per SM of the batched kernel (its register
+// budget): 4 for every class, from a sweep on B200 (icosphere, One-Weekend,
+// SDF-field and Cornell views); overridden by rb_server_opts.occupancy /
+// rb_render_opts.reserved[0].
+static int batch_minb(int ms, bool nee) {
+  (void)ms;
+  (void)nee;
+  return 4;
 }
 
 // One persistent launch for a class group; the next-event-estimation variant
@@ -237,9 +248,11 @@ static void preload_ms() {
   cudaFuncGetAttributes(&a, k_batch<MS, 1, false>);
   cudaFuncGetAttributes(&a, k_batch<MS, 2, false>);
   cudaFuncGetAttributes(&a, k_batch<MS, 3, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, false>);
   cudaFuncGetAttributes(&a, k_batch<MS, 1, true>);
   cudaFuncGetAttributes(&a, k_batch<MS, 2, true>);
   cudaFuncGetAttributes(&a, k_batch<MS, 3, true>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, true>);
 }
 static void preload_batch_kernels() {
   preload_ms<RB_MS_DIFFUSE>();
@@ -496,7 +509,7 @@ static int server_step(Server &S) {
   const bool frames = S.o.frames_every > 0;
   auto minb_of = [&](int grp) {
     (void)grp;
-    return S.o.occupancy > 0 ? std::min(S.o.occupancy, 3) : 2;  // 2 resident blocks: tuned on B200
+    return S.o.occupancy > 0 ? std::min(S.o.occupancy, 4) : batch_minb(grp > 4 ? grp - 4 : grp, grp > 4);
   };
   auto launch_group = [&](int grp) {
     const int cls = grp > 4 ? grp - 4 : grp;
@@ -998,7 +1011,7 @@ int rb_render_views(const rb_cuda_scene *scene, int n_views, int width, int heig
       !cuda_ok(cudaEventRecord(T.uploaded, st), "rb_render_views: event"))
     return RB_ERR_CUDA;
   const rb_render_opts o = current_opts();
-  const int minb = o.reserved[0] > 0 ? std::min(o.reserved[0], 3) : 2;
+  const int minb = o.reserved[0] > 0 ? std::min(o.reserved[0], 4) : batch_minb(ds->ms, G.nee != 0);
   BatchCtl *d_ctl = reinterpret_cast<BatchCtl *>(T.d);
   launch_batch(ds->ms, minb, G.nee != 0, st, reinterpret_cast<const BatchJob *>(T.d + sizeof(BatchCtl)), d_ctl, sms);
   if (!cuda_ok(cudaGetLastError(), "rb_render_views: launch")) return RB_ERR_CUDA;

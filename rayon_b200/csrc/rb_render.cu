@@ -678,17 +678,17 @@ int launch_primary(const DeviceScene *ds, const FrameF &P, int32_t *ids, float *
 // class; rb_render_opts.reserved[0] overrides it (the autotuner's knob).
 // Defaults from a sweep on B200 (occupancy x block shape, per class).
 static int default_minb(int ms, bool nee) {
-  if (ms == RB_MS_DIFFUSE) return 4;
-  if (ms == RB_MS_CLASSIC) return 2;
-  return nee ? 1 : 2;
+  if (ms == RB_MS_DIFFUSE || ms == RB_MS_CLASSIC) return 4;
+  if (ms == RB_MS_FULL) return nee ? 2 : 4;
+  return 2;  // SDF
 }
 static void default_block(int ms, int &bx, int &by) {
-  if (ms == RB_MS_SDF || ms == RB_MS_DIFFUSE) {  // 8x8 tiles: a warp's rays stay close together
-    bx = by = 8;
+  if (ms == RB_MS_CLASSIC) {
+    bx = 16;
+    by = 8;
     return;
   }
-  bx = ms >= RB_MS_FULL ? 32 : 16;
-  by = ms >= RB_MS_FULL ? 4 : 8;
+  bx = by = 8;  // 8x8 tiles: a warp's rays stay close together
 }
 
 template <bool NEE, int MS>
