@@ -269,7 +269,11 @@ typedef struct rb_render_opts {
   uint32_t seed;      /* RNG seed of the per-path counter-based streams     */
   int block_x, block_y; /* launch shape of the per-pixel kernel (0 = tuned per class) */
   int reserved[4];      /* [0]: resident 256-thread blocks per SM the kernel is
-                           compiled for (1-4; 0 = tuned per material class) */
+                           compiled for (1-4; 0 = tuned per material class);
+                           [1]: sample slices per pixel of the per-pixel kernel
+                           (0 = automatic: frames with fewer pixels than four
+                           times the GPU's resident threads split their samples,
+                           up to 8 slices) */
 } rb_render_opts;
 void rb_get_render_opts(rb_render_opts *out);
 void rb_set_render_opts(const rb_render_opts *in);

@@ -218,3 +218,32 @@ def test_grouped_layout_renders_the_same(cuda, name):
         assert bad.mean() < 0.005, (g, bad.mean())
         grp.free()
     lin.free()
+
+
+def test_sample_slices_render_the_same(cuda):
+    # a small frame splits its samples over several threads per pixel; the
+    # samples (streams) are the same, only the FP32 summation grouping differs
+    import ctypes as C
+
+    from rayon_b200 import lib
+    from rayon_b200._native import RenderOpts
+    spec, _ = _cases()["one_weekend"]
+    w, h, spp = 40, 24, 32
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds = sc.upload()
+    fr = spec.camera.frame(w, h)
+    out = {}
+    for slices in (1, 4, 5):
+        o = RenderOpts()
+        lib.rb_get_render_opts(C.byref(o))
+        o.reserved[1] = slices
+        lib.rb_set_render_opts(C.byref(o))
+        out[slices], cnt = render.render_accumulate(ds, fr, w, h, spp, spec.depth, background=spec.background,
+                                                    dof=spec.dof, counters=True)
+        assert int(cnt[1]) == w * h * spp
+        o.reserved[1] = 0
+        lib.rb_set_render_opts(C.byref(o))
+    for slices in (4, 5):
+        np.testing.assert_allclose(out[slices], out[1], rtol=1e-4, atol=1e-4 * spp)
+    ds.free()
