@@ -741,6 +741,31 @@ static void launch_ms(int minb, dim3 grd, dim3 blk, size_t sm, cudaStream_t st, 
   }
 }
 
+// Stream-ordered scratch of the sample slices: a private memory pool per
+// device that keeps its memory between calls (the default pool returns freed
+// memory at every synchronisation, and mapping it again stalls the stream).
+static cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (!cuda_ok(cudaMemPoolCreate(&p, &props), "slice scratch pool")) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, int *counts,
                   unsigned long long *counters, cudaStream_t st) {
   const rb_render_opts o = current_opts();
@@ -775,8 +800,10 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
     }
   }
   float4 *part = nullptr;
-  if (slices > 1 &&
-      !cuda_ok(cudaMallocAsync((void **)&part, sizeof(float4) * (size_t)npix * (slices - 1), st), "slice scratch"))
+  cudaMemPool_t pool = slices > 1 ? scratch_pool() : nullptr;
+  if (slices > 1 && (!pool || !cuda_ok(cudaMallocFromPoolAsync((void **)&part,
+                                                               sizeof(float4) * (size_t)npix * (slices - 1), pool, st),
+                                       "slice scratch")))
     slices = 1;
   grd.z = slices;
 #define RB_LAUNCH(NEE_, MS_) \
