@@ -538,6 +538,15 @@ struct WfEngine {
   WfJob *h_jobs = nullptr;
   WfJob *d_jobs = nullptr;
   int jobs_cap = 0;
+  // the last run's 8-iteration graph, reused while its launch parameters (the
+  // bytes of key) are the same: a serving loop runs the engine every iteration
+  struct GraphKey {
+    WfParams W;
+    int march_grid;
+    int variant;
+  } key;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t fence = nullptr;
 };
 
 static void wf_free(WfEngine &E) {
@@ -556,6 +565,8 @@ static void wf_free(WfEngine &E) {
   cudaFree(E.d_jobs);
   E.h_jobs = E.d_jobs = nullptr;
   E.jobs_cap = 0;
+  if (E.graph) cudaGraphExecDestroy(E.graph);
+  E.graph = nullptr;
 }
 
 static bool wf_alloc_march(WfEngine &E) {
@@ -618,29 +629,43 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   }
   k_wf_fill<<<grid, 256, 0, st>>>(W, E.q[0], 0, E.capacity);
   g_launches++;
-  // eight iterations per graph (queues 0->1->0 ...), replayed until empty
-  cudaGraph_t g = nullptr;
-  cudaGraphExec_t ge = nullptr;
-  if (!cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "wavefront capture")) return RB_ERR_CUDA;
-  for (int i = 0; i < 8; ++i) wf_iteration<MS, NEE>(W, E, i & 1, grid, march_grid, st);
-  const cudaError_t ec = cudaStreamEndCapture(st, &g);  // always end the capture, also after an error
-  if (!cuda_ok(ec, "wavefront capture") || !g) return RB_ERR_CUDA;
-  const bool inst = cuda_ok(cudaGraphInstantiate(&ge, g, 0), "wavefront graph");
-  cudaGraphDestroy(g);
-  if (!inst) return RB_ERR_CUDA;
+  // eight iterations per graph (queues 0->1->0 ...), replayed until empty;
+  // the graph is kept for the next run with the same launch parameters
+  WfEngine::GraphKey key;
+  std::memset(&key, 0, sizeof key);
+  std::memcpy(&key.W, &W, sizeof W);
+  key.march_grid = march_grid;
+  key.variant = MS * 2 + (NEE ? 1 : 0);
+  if (!E.graph || std::memcmp(&key, &E.key, sizeof key) != 0) {
+    if (E.graph) cudaGraphExecDestroy(E.graph);
+    E.graph = nullptr;
+    cudaGraph_t g = nullptr;
+    if (!cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "wavefront capture"))
+      return RB_ERR_CUDA;
+    for (int i = 0; i < 8; ++i) wf_iteration<MS, NEE>(W, E, i & 1, grid, march_grid, st);
+    const cudaError_t ec = cudaStreamEndCapture(st, &g);  // always end the capture, also after an error
+    if (!cuda_ok(ec, "wavefront capture") || !g) return RB_ERR_CUDA;
+    const bool inst = cuda_ok(cudaGraphInstantiate(&E.graph, g, 0), "wavefront graph");
+    cudaGraphDestroy(g);
+    if (!inst) {
+      E.graph = nullptr;
+      return RB_ERR_CUDA;
+    }
+    std::memcpy(&E.key, &key, sizeof key);
+  }
   int it = 0;
   for (int guard = 0; guard < 1 << 20; ++guard) {
-    cudaGraphLaunch(ge, st);
+    cudaGraphLaunch(E.graph, st);
     g_launches += march_grid > 0 ? 32 : 24;
     it += 8;
     cudaMemcpyAsync(E.h_ctl, E.ctl, sizeof(WfCtl), cudaMemcpyDeviceToHost, st);
     if (!cuda_ok(cudaStreamSynchronize(st), "wavefront iteration")) {
-      cudaGraphExecDestroy(ge);
+      cudaGraphExecDestroy(E.graph);
+      E.graph = nullptr;
       return RB_ERR_CUDA;
     }
     if (E.h_ctl->count[0] == 0) break;  // eight iterations end in queue 0
   }
-  cudaGraphExecDestroy(ge);
   if (iterations) *iterations = it;
   return RB_OK;
 }
@@ -707,8 +732,9 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
     W.list = E.list;
     W.cap = E.capacity;
   }
-  cudaEvent_t fence;
-  if (!cuda_ok(cudaEventCreateWithFlags(&fence, cudaEventDisableTiming), "wavefront fence")) return RB_ERR_CUDA;
+  if (!E.fence && !cuda_ok(cudaEventCreateWithFlags(&E.fence, cudaEventDisableTiming), "wavefront fence"))
+    return RB_ERR_CUDA;
+  cudaEvent_t fence = E.fence;
   cudaEventRecord(fence, caller);
   cudaStreamWaitEvent(st, fence, 0);
   cudaMemcpyAsync(E.d_jobs, E.h_jobs, sizeof(WfJob) * njobs, cudaMemcpyHostToDevice, st);
@@ -732,7 +758,6 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
   cudaEventRecord(fence, st);
   cudaStreamWaitEvent(caller, fence, 0);
   cudaStreamSynchronize(st);
-  cudaEventDestroy(fence);
   return rc;
 }
 
