@@ -89,20 +89,21 @@ def render_accumulate(ds, frame, w: int, h: int, spp: int, depth: int, backgroun
     """Per-pixel radiance sums (h, w, 3) float64 of samples [sample_base, sample_base + spp)."""
     torch = _torch()
     set_globals(light=light, background=background, fuzz=fuzz, glass_ior=glass_ior, dof=dof)
-    acc = torch.zeros((w * h, 4), dtype=torch.float32, device="cuda")
-    comp = torch.zeros((w * h, 4), dtype=torch.float32, device="cuda") if kahan else None
-    cnt = torch.zeros(4, dtype=torch.int64, device="cuda")
+    # sums, then Kahan compensations, in one allocation (one fill, one copy back)
+    buf = torch.zeros((2 if kahan else 1, w * h, 4), dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(4, dtype=torch.int64, device="cuda") if counters else None
     fr = np.ascontiguousarray(frame, np.float64)
     with options(nee=nee, seed=seed):
         check(lib.rb_render_accumulate(ds.handle, w, h, fr.ctypes.data_as(C.POINTER(C.c_double)), spp, sample_base,
-                                       depth, C.c_void_p(acc.data_ptr()),
-                                       C.c_void_p(comp.data_ptr()) if comp is not None else None,
-                                       C.c_void_p(cnt.data_ptr()), _stream_ptr()), "rb_render_accumulate")
-        torch.cuda.synchronize()
-    out = acc[:, :3].double()
-    if comp is not None:
-        out = out - comp[:, :3].double()  # Kahan: true sum = sum - compensation
-    img = out.cpu().numpy().reshape(h, w, 3)
+                                       depth, C.c_void_p(buf[0].data_ptr()),
+                                       C.c_void_p(buf[1].data_ptr()) if kahan else None,
+                                       C.c_void_p(cnt.data_ptr()) if cnt is not None else None, _stream_ptr()),
+              "rb_render_accumulate")
+        host = buf.cpu().numpy()  # synchronises the stream
+    img = host[0, :, :3].astype(np.float64)
+    if kahan:
+        img -= host[1, :, :3]  # Kahan: true sum = sum - compensation
+    img = img.reshape(h, w, 3)
     set_globals()
     if counters:
         return img, cnt.cpu().numpy()
