@@ -291,6 +291,17 @@ bool prim_t(const Scene &S, int i, const Ray &r, double tmin, double tmax, doubl
 // on the field's magnitude, each step clamped to the next window entry;
 // normal by central differences (step 5e-4) over the hit point's windows;
 // material of the nearest primitive.
+//
+// Convex skip: where one window alone holds t and its primitive is convex
+// (sphere, box, rounded box, capsule), the field is that primitive's distance,
+// a convex function of t. Once it has grown between two consecutive steps
+// (by more than a quarter, so FP32 rounding near the surface cannot fake the
+// growth) it keeps growing, so no hit lies before the next window entry: the
+// march jumps there, as it would have arrived after enough steps.
+bool sdf_convex(int type) {
+  return type == RB_SDF_SPHERE || type == RB_SDF_BOX || type == RB_SDF_ROUND_BOX || type == RB_SDF_CAPSULE;
+}
+
 bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &tt, D3 &n, int &mat) {
   struct Win { int idx; double t0, t1; };
   std::vector<Win> c;
@@ -306,13 +317,17 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
   }
   if (c.empty()) return false;
   const double FAR = 1e30;
+  int held = 0, lone = -1;  // windows holding t at the last evaluation; the last of them
   auto field = [&](const D3 &p, double t, double &next, int *nearest) {
     double F = FAR, best = FAR;
     bool first = true;
     next = FAR;
+    held = 0;
     for (const Win &w : c) {
       if (w.t0 > t) { next = std::fmin(next, w.t0); continue; }
       if (t > w.t1) continue;
+      ++held;
+      lone = w.idx;
       const double d = sdf_eval1(S.sdf[w.idx], p);
       if (nearest && d < best) { best = d; *nearest = w.idx; }
       F = first ? d : smin_poly(F, d, S.sdf_k);
@@ -328,12 +343,15 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
     f0 = field(r.at(t), t, next, nullptr);
   }
   const double sgn = f0 < 0 ? -1.0 : 1.0;
+  int prev = -1;  // lone convex primitive of the previous step, and its distance there
+  double prev_d = 0;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const D3 p = r.at(t);
     const double raw = field(p, t, next, nullptr);
     if (raw == FAR) {
       if (next == FAR || next > tmax) return false;
       t = next;
+      prev = -1;
       continue;
     }
     const double F = sgn * raw;
@@ -351,6 +369,15 @@ bool sdf_field(const Scene &S, const Ray &r, double tmin, double tmax, double &t
       tt = t;
       return true;
     }
+    const int one = (sgn > 0 && held == 1 && sdf_convex(S.sdf[lone].type)) ? lone : -1;
+    if (one >= 0 && one == prev && raw > 1.25 * prev_d) {  // convex skip
+      if (next == FAR || next > tmax) return false;
+      t = next;
+      prev = -1;
+      continue;
+    }
+    prev = one;
+    prev_d = raw;
     t = std::fmin(t + F * il, next);
     if (t > tmax) return false;
   }

@@ -297,6 +297,10 @@ struct Server {
   BatchCtl *d_ctl = nullptr;
   unsigned long long *h_conv = nullptr, *d_conv = nullptr;  // converged-pixel counts per planned job
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // wavefront jobs run on their own stream beside the class kernels: ev_up
+  // marks the iteration's uploads, ev_wf the end of its wavefront runs
+  cudaStream_t st_wf = nullptr;
+  cudaEvent_t ev_up = nullptr, ev_wf = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_frames = -1;
   double aging = 0.5;  // priority = remaining paths / (1 + aging * seconds waited)
@@ -540,7 +544,7 @@ static int server_step(Server &S) {
         wj.push_back(w);
       }
       uint64_t c[4] = {0, 0, 0, 0};
-      const int rc = wf_render_jobs(S.scenes[sc], wj.data(), (int)wj.size(), 1 << 22, c, S.st);
+      const int rc = wf_render_jobs(S.scenes[sc], wj.data(), (int)wj.size(), 1 << 22, c, S.st_wf);
       if (rc != RB_OK) return rc;
       wf_segments += c[0];
       wf_paths += c[1];
@@ -574,9 +578,16 @@ static int server_step(Server &S) {
     cudaEventRecord(S.ev0, S.st);
     cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
     cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
+    cudaEventRecord(S.ev_up, S.st);
     kernels(false);
     if (!wf_k.empty()) {
+      // the wavefront jobs touch only their own sums, so they start after the
+      // uploads and run beside the class kernels (their blocks take the SMs
+      // the class kernels' tails leave idle); the iteration ends after both
+      cudaStreamWaitEvent(S.st_wf, S.ev_up, 0);
       const int rc = run_wavefront();
+      cudaEventRecord(S.ev_wf, S.st_wf);
+      cudaStreamWaitEvent(S.st, S.ev_wf, 0);
       if (rc != RB_OK) return rc;
     }
     if (frames) {
@@ -725,6 +736,12 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   preload_batch_kernels();
   cudaEventCreate(&S.ev0);
   cudaEventCreate(&S.ev1);
+  if (!cuda_ok(cudaStreamCreateWithFlags(&S.st_wf, cudaStreamNonBlocking), "server wavefront stream") ||
+      !cuda_ok(cudaEventCreateWithFlags(&S.ev_up, cudaEventDisableTiming), "server event") ||
+      !cuda_ok(cudaEventCreateWithFlags(&S.ev_wf, cudaEventDisableTiming), "server event")) {
+    rb_server_destroy(r);
+    return nullptr;
+  }
   std::memset(&S.stats, 0, sizeof S.stats);
   S.quantum = S.o.paths_per_iteration;
   S.t0 = std::chrono::steady_clock::now();
@@ -746,6 +763,12 @@ void rb_server_destroy(rb_server *r) {
   if (S.d_conv) cudaFree(S.d_conv);
   if (S.ev0) cudaEventDestroy(S.ev0);
   if (S.ev1) cudaEventDestroy(S.ev1);
+  if (S.st_wf) {
+    cudaStreamSynchronize(S.st_wf);
+    cudaStreamDestroy(S.st_wf);
+  }
+  if (S.ev_up) cudaEventDestroy(S.ev_up);
+  if (S.ev_wf) cudaEventDestroy(S.ev_wf);
   if (S.own_stream && S.st) cudaStreamDestroy(S.st);
   delete r;
 }

@@ -269,6 +269,8 @@ static __device__ float sdf_march_prim(const SceneView &S, int prim, const Ray &
 // of those is sphere-traced after the traversal.
 #define RB_SDF_CAND 24
 static_assert(RB_SDF_CAND <= 32, "field folds mark candidates in a 32-bit mask");
+// idx[i] is a candidate code: (SDF table index << 1) | 1 when the primitive is
+// convex. Codes order as their indices do.
 struct SdfCand {
   int n;
   int idx[RB_SDF_CAND];
@@ -299,7 +301,7 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
         const float sq = sqrtf(disc);
         const float t0 = (-hb - sq) / aa, t1 = (-hb + sq) / aa;
         if (t1 >= tmin && t0 <= tmax && cand->n < RB_SDF_CAND) {
-          cand->idx[cand->n] = __float_as_int(__ldg(p + 1).x);
+          cand->idx[cand->n] = (__float_as_int(b.x) << 1) | (__float_as_int(b.y) & 1);
           cand->t0[cand->n] = t0;
           cand->t1[cand->n] = t1;
           ++cand->n;

@@ -226,6 +226,9 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
       const double pad = hs.sdf.blend_k + 1e-3;
       put(r, 0, q.px); put(r, 1, q.py); put(r, 2, q.pz); put(r, 3, (float)(bound * 1.0001 + pad));
       put(r, 4, __int_as_float_host((int)L.sdf.size()));
+      // convex primitives (their distance is convex along a ray) allow the field march's convex skip
+      const bool convex = t == RB_SDF_SPHERE || t == RB_SDF_BOX || t == RB_SDF_ROUND_BOX || t == RB_SDF_CAPSULE;
+      put(r, 5, __int_as_float_host(convex ? 1 : 0));
       L.sdf.push_back(q);
       put(r, 11, __uint_as_float_host(tag_of(g, kind)));
     }

@@ -514,13 +514,25 @@ __device__ __forceinline__ float smin_poly(float d1, float d2, float k) {
 // hit below S.sdf_eps; outward normal by central differences with a 5e-4 step
 // over the hit point's window set; the material is that of the nearest
 // primitive.
+//
+// Convex skip: where one window alone holds t and its primitive is convex
+// (sphere, box, rounded box, capsule), the field is that primitive's distance,
+// a convex function of t. Once it has grown between two consecutive steps by
+// more than a quarter (a margin FP32 rounding near the surface cannot fake),
+// it keeps growing, so no hit lies before the next window entry and the march
+// jumps there (where it would have arrived, clamped, after more steps). Rays
+// leaving a surface and rays past their closest approach stop crawling.
 #define RB_SDF_NORMAL_EPS 5e-4f
 #define RB_SDF_FAR 1e30f
+#ifndef RB_SDF_SKIP_GROWTH
+#define RB_SDF_SKIP_GROWTH 1.25f
+#endif
 // Field at p = r.at(t) over the windows holding t; `next` is the nearest
 // window entry beyond t (RB_SDF_FAR when none). RB_SDF_FAR when no window
-// holds t.
+// holds t. `lone` (optional) gets the candidate code of the only window
+// holding t, -1 when none or several do.
 __device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCand &c, const f3 &p, float t,
-                                                float &next, int *nearest) {
+                                                float &next, int *nearest, int *lone = nullptr) {
   // two passes so that a warp's lanes evaluate together: mark the candidates
   // whose window holds t (index order), then fold the marked ones
   uint32_t active = 0;
@@ -530,15 +542,17 @@ __device__ __forceinline__ float sdf_field_eval(const SceneView &S, const SdfCan
     if (t0 > t) next = fminf(next, t0);
     else if (t <= c.t1[i]) active |= 1u << i;
   }
+  if (lone) *lone = (active != 0u && (active & (active - 1u)) == 0u) ? c.idx[__ffs(active) - 1] : -1;
   float F = RB_SDF_FAR, best = RB_SDF_FAR;
   bool first = true;
   while (active) {
     const int i = __ffs(active) - 1;
     active &= active - 1;
-    const float d = sdf_eval_at(S.sdf, c.idx[i], p);
+    const int id = c.idx[i] >> 1;
+    const float d = sdf_eval_at(S.sdf, id, p);
     if (nearest && d < best) {
       best = d;
-      *nearest = c.idx[i];
+      *nearest = id;
     }
     F = first ? d : smin_poly(F, d, S.sdf_k);
     first = false;
@@ -569,21 +583,26 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
   sdf_sort_cand(c);
   const float inv_len = 1.0f / r.d.length();
   float t = tmin, next;
+  int lone = -1;
   // a ray that starts in the eps shell around the surface (a bounce off the
   // field) first steps out of it, so the inside/outside decision is made
   // where the field is clearly signed
-  float f0 = sdf_field_eval(S, c, r.at(t), t, next, nullptr);
-  for (int k = 0; k < 8 && fabsf(f0) < 2.0f * S.sdf_eps; ++k) {
+  float raw = sdf_field_eval(S, c, r.at(t), t, next, nullptr, &lone);
+  for (int k = 0; k < 8 && fabsf(raw) < 2.0f * S.sdf_eps; ++k) {
     t += 2.0f * S.sdf_eps * inv_len;
-    f0 = sdf_field_eval(S, c, r.at(t), t, next, nullptr);
+    raw = sdf_field_eval(S, c, r.at(t), t, next, nullptr, &lone);
   }
-  const float sgn = f0 < 0.0f ? -1.0f : 1.0f;
+  const float sgn = raw < 0.0f ? -1.0f : 1.0f;
+  int prev = -1;  // lone convex candidate of the previous step, and the field there
+  float prev_d = 0.0f;
   for (int i = 0; i < S.sdf_steps; ++i) {
     const f3 p = r.at(t);
-    const float raw = sdf_field_eval(S, c, p, t, next, nullptr);
+    // the last escape evaluation is the first step's
+    if (i > 0) raw = sdf_field_eval(S, c, p, t, next, nullptr, &lone);
     if (raw == RB_SDF_FAR) {  // between windows: jump to the next entry
       if (next == RB_SDF_FAR || next > tmax) return false;
       t = next;
+      prev = -1;
       continue;
     }
     const float F = sgn * raw;
@@ -599,12 +618,21 @@ static __device__ __noinline__ bool sdf_field_march(const SceneView &S, const Ra
                      sdf_field_eval(S, c, p - f3(0, 0, e), t, nx, nullptr));
       const float gl = g.length();
       n_out = gl > 0.0f ? g / gl : f3(0.0f, 1.0f, 0.0f);
-      int nearest = c.idx[0];
+      int nearest = c.idx[0] >> 1;
       sdf_field_eval(S, c, p, t, nx, &nearest);
       mat_out = S.sdf[nearest].material;
       t_out = t;
       return true;
     }
+    const int one = (sgn > 0.0f && lone >= 0 && (lone & 1)) ? lone : -1;
+    if (one >= 0 && one == prev && raw > RB_SDF_SKIP_GROWTH * prev_d) {  // convex skip
+      if (next == RB_SDF_FAR || next > tmax) return false;
+      t = next;
+      prev = -1;
+      continue;
+    }
+    prev = one;
+    prev_d = raw;
     t = fminf(t + F * inv_len, next);
     if (t > tmax) return false;
   }

@@ -188,7 +188,7 @@ __device__ __forceinline__ int4 wf_cand(const WfParams &W, const int4 (&cr)[WF_C
 // same time, k = 0, 1, ... (the fold order per lane is still index order).
 __device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, const float4 *tab, int slot, int n,
                                           const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
-                                          int *nearest) {
+                                          int *nearest, int &lone) {
   uint32_t active = 0;
   float nx = RB_SDF_FAR;
   for (int i = 0; i < n; ++i) {
@@ -198,12 +198,16 @@ __device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W,
     else if (t <= __int_as_float(e.z)) active |= 1u << i;
   }
   next = nx;
+  const bool single = active != 0u && (active & (active - 1u)) == 0u;
+  lone = -1;
   float F = RB_SDF_FAR, best = RB_SDF_FAR;
   bool first = true;
   while (active) {
     const int i = __ffs(active) - 1;
     active &= active - 1;
-    const int id = wf_cand(W, cr, slot, i).x;
+    const int code = wf_cand(W, cr, slot, i).x;
+    if (single) lone = code;
+    const int id = code >> 1;
     const float d = tab ? sdf_eval_words(tab[5 * id], tab[5 * id + 1], tab[5 * id + 2], tab[5 * id + 3],
                                          tab[5 * id + 4], p)
                         : sdf_eval_at(S.sdf, id, p);
@@ -220,8 +224,9 @@ __device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W,
 // Persistent field march over the march list. Every pass, each busy lane
 // evaluates the field exactly once, whatever its phase, so the warp's lanes
 // evaluate in lockstep: escape (stepping out of the eps shell, up to 8
-// passes), march (one sphere-tracing step of sdf_field_march's loop) and, at
-// a hit, the six central differences of the normal (one per pass). The
+// passes), march (one sphere-tracing step of sdf_field_march's loop, its
+// convex skip included) and, at a hit, the six central differences of the
+// normal (one per pass). The
 // nearest primitive (the hit's material) is tracked in every march
 // evaluation, which at the hit is the evaluation at the hit point itself. A
 // lane whose ray finishes (hit, windows left behind, closest primitive hit
@@ -229,8 +234,14 @@ __device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W,
 // warp). A field hit replaces the ray's hit record.
 enum : int { WF_ESCAPE = 0, WF_MARCH = 1, WF_NORMAL = 2 };
 
+// Four resident 256-thread blocks per SM (64 registers, a few bytes spilled):
+// the march is latency-bound, and 50 % occupancy beat 37.5 % by 7 % on the
+// SDF field.
+#ifndef WF_MARCH_MINB
+#define WF_MARCH_MINB 4
+#endif
 template <int MS>
-__global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int stage_table) {
+__global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQueue q, int stage_table) {
   extern __shared__ float4 s_tab[];
   const int lane = threadIdx.x & 31;
   const SceneView &S = W.S;
@@ -243,7 +254,8 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int sta
   const float4 *tab = stage_table ? s_tab : nullptr;
   const unsigned total = (unsigned)W.ctl->march_count;
   const float e = RB_SDF_NORMAL_EPS;
-  int slot = 0, n = 0, steps = 0, phase = WF_ESCAPE, sub = 0, nearest = 0;
+  int slot = 0, n = 0, steps = 0, phase = WF_ESCAPE, sub = 0, nearest = 0, prev = -1;
+  float prev_d = 0.f;
   int4 cr[WF_CAND_REG];
 #pragma unroll
   for (int i = 0; i < WF_CAND_REG; ++i) cr[i] = make_int4(0, 0, 0, 0);
@@ -278,6 +290,7 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int sta
           phase = WF_ESCAPE;
           sub = 0;
           steps = 0;
+          prev = -1;
           busy = true;
         } else {
           drained = true;
@@ -296,8 +309,8 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int sta
       pe = r.at(t);
     }
     float next;
-    int near = cr[0].x;
-    const float raw = wf_field(S, W, tab, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near);
+    int near = cr[0].x >> 1, lone;
+    const float raw = wf_field(S, W, tab, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near, lone);
     bool finished = false;
     if (phase == WF_NORMAL) {
       if (sub & 1) {
@@ -330,6 +343,7 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int sta
         if (raw == RB_SDF_FAR) {  // between windows: jump to the next entry
           if (next == RB_SDF_FAR || next > tmax) finished = true;
           else t = next;
+          prev = -1;
         } else {
           const float F = sgn * raw;
           if (F < S.sdf_eps) {
@@ -342,8 +356,17 @@ __global__ void __launch_bounds__(256) k_wf_march(WfParams W, WfQueue q, int sta
               finished = true;
             }
           } else {
-            t = fminf(t + F * inv_len, next);
-            if (t > tmax) finished = true;
+            const int one = (sgn > 0.0f && lone >= 0 && (lone & 1)) ? lone : -1;
+            if (one >= 0 && one == prev && raw > RB_SDF_SKIP_GROWTH * prev_d) {  // convex skip
+              if (next == RB_SDF_FAR || next > tmax) finished = true;
+              else t = next;
+              prev = -1;
+            } else {
+              prev = one;
+              prev_d = raw;
+              t = fminf(t + F * inv_len, next);
+              if (t > tmax) finished = true;
+            }
           }
         }
         if (!finished && phase == WF_MARCH && ++steps >= S.sdf_steps) finished = true;
