@@ -61,6 +61,12 @@ struct BatchCtl {
   int pad[4];
 };
 
+// The scene and settings shared by every job of one batched launch.
+struct BatchUniform {
+  SceneView S;
+  Globals G;
+};
+
 __device__ __forceinline__ int find_job(const BatchJob *__restrict__ jobs, int njobs, long long t) {
   int lo = 0, hi = njobs - 1;
   while (lo < hi) {
@@ -71,8 +77,18 @@ __device__ __forceinline__ int find_job(const BatchJob *__restrict__ jobs, int n
   return lo;
 }
 
-template <int MS, int MINB, bool NEE>
-__global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict__ jobs, BatchCtl *__restrict__ ctl) {
+// Scene and settings of a lane's job: the launch's own (kernel parameters,
+// read through the constant bank) when every job of the launch shares them
+// (UNI), else the job table's record (global loads every path segment).
+template <bool UNI, class T>
+__device__ __forceinline__ const T &job_or_uniform(const T &uniform, const T &job) {
+  if constexpr (UNI) return uniform;
+  else return job;
+}
+
+template <int MS, int MINB, bool NEE, bool UNI>
+__global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict__ jobs, BatchCtl *__restrict__ ctl,
+                                                     const SceneView Su, const Globals Gu) {
   extern __shared__ int2 smem[];
   jobs += ctl->job_offset;
   const int tid = threadIdx.x;
@@ -126,7 +142,7 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
         if (s < nsamp && J.P.max_depth > 0) {
           key = rb_path_key(J.P.seed, J.P.salt, (uint32_t)pix, (uint32_t)(J.P.sample_base + s));
           ++s;
-          ray = camera_ray(J.P, J.G, x, y, key);
+          ray = camera_ray(J.P, job_or_uniform<UNI>(Gu, J.G), x, y, key);
           thr = f3(1.f, 1.f, 1.f);
           L = f3(0.f, 0.f, 0.f);
           bounce = 0;
@@ -156,7 +172,8 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
       }
       if (alive) {
         ++segs;
-        if (path_segment<NEE, MS>(J.S, J.G, st, ovf, ray, thr, L, bounce, prev_pdf, key, J.P.max_depth)) {
+        if (path_segment<NEE, MS>(job_or_uniform<UNI>(Su, J.S), job_or_uniform<UNI>(Gu, J.G), st, ovf, ray, thr, L,
+                                  bounce, prev_pdf, key, J.P.max_depth)) {
           kahan_add(sx, cx, L.x);
           kahan_add(sy, cy, L.y);
           kahan_add(sz, cz, L.z);
@@ -202,13 +219,24 @@ __global__ void k_batch_frames(const BatchJob *__restrict__ jobs, const BatchCtl
 }
 
 template <int MS, bool NEE>
-static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl) {
+// uni (may be null): the scene and settings every job of the launch shares;
+// the uniform variant exists for the default occupancy (4 blocks per SM).
+static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl,
+                            const BatchUniform *uni) {
   const size_t sm = sizeof(int2) * RB_SHORT * 256;
+  if (uni && minb == 4) {
+    k_batch<MS, 4, NEE, true><<<grid, 256, sm, st>>>(jobs, ctl, uni->S, uni->G);
+    return;
+  }
+  SceneView s0;
+  Globals g0;
+  std::memset(&s0, 0, sizeof s0);
+  std::memset(&g0, 0, sizeof g0);
   switch (minb) {
-    case 1: k_batch<MS, 1, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    case 3: k_batch<MS, 3, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    case 4: k_batch<MS, 4, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
-    default: k_batch<MS, 2, NEE><<<grid, 256, sm, st>>>(jobs, ctl); break;
+    case 1: k_batch<MS, 1, NEE, false><<<grid, 256, sm, st>>>(jobs, ctl, s0, g0); break;
+    case 3: k_batch<MS, 3, NEE, false><<<grid, 256, sm, st>>>(jobs, ctl, s0, g0); break;
+    case 4: k_batch<MS, 4, NEE, false><<<grid, 256, sm, st>>>(jobs, ctl, s0, g0); break;
+    default: k_batch<MS, 2, NEE, false><<<grid, 256, sm, st>>>(jobs, ctl, s0, g0); break;
   }
 }
 
@@ -224,18 +252,19 @@ static int batch_minb(int ms, bool nee) {
 
 // One persistent launch for a class group; the next-event-estimation variant
 // only when a job of the group asks for it (it costs registers).
-static void launch_batch(int ms, int minb, bool nee, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms) {
+static void launch_batch(int ms, int minb, bool nee, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms,
+                         const BatchUniform *uni) {
   const int grid = sms * minb;  // persistent: exactly the resident blocks
   if (nee) {
-    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, true>(minb, grid, st, jobs, ctl);
-    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, true>(minb, grid, st, jobs, ctl);
-    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, true>(minb, grid, st, jobs, ctl);
-    else launch_batch_ms<RB_MS_SDF, true>(minb, grid, st, jobs, ctl);
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, true>(minb, grid, st, jobs, ctl, uni);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, true>(minb, grid, st, jobs, ctl, uni);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, true>(minb, grid, st, jobs, ctl, uni);
+    else launch_batch_ms<RB_MS_SDF, true>(minb, grid, st, jobs, ctl, uni);
   } else {
-    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, false>(minb, grid, st, jobs, ctl);
-    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, false>(minb, grid, st, jobs, ctl);
-    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, false>(minb, grid, st, jobs, ctl);
-    else launch_batch_ms<RB_MS_SDF, false>(minb, grid, st, jobs, ctl);
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, false>(minb, grid, st, jobs, ctl, uni);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, false>(minb, grid, st, jobs, ctl, uni);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, false>(minb, grid, st, jobs, ctl, uni);
+    else launch_batch_ms<RB_MS_SDF, false>(minb, grid, st, jobs, ctl, uni);
   }
   g_launches++;
 }
@@ -245,14 +274,16 @@ static void launch_batch(int ms, int minb, bool nee, cudaStream_t st, const Batc
 template <int MS>
 static void preload_ms() {
   cudaFuncAttributes a;
-  cudaFuncGetAttributes(&a, k_batch<MS, 1, false>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 2, false>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 3, false>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 4, false>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 1, true>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 2, true>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 3, true>);
-  cudaFuncGetAttributes(&a, k_batch<MS, 4, true>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 1, false, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 2, false, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 3, false, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, false, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, false, true>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 1, true, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 2, true, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 3, true, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, true, false>);
+  cudaFuncGetAttributes(&a, k_batch<MS, 4, true, true>);
 }
 static void preload_batch_kernels() {
   preload_ms<RB_MS_DIFFUSE>();
@@ -303,6 +334,10 @@ struct Server {
   cudaEvent_t ev_up = nullptr, ev_wf = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_frames = -1;
+  // per class group: the scene shared by all its jobs (-1: none or several)
+  // and their shared settings, as the graph's kernels were captured with
+  int graph_scene[RB_GROUPS];
+  Globals graph_G[RB_GROUPS];
   double aging = 0.5;  // priority = remaining paths / (1 + aging * seconds waited)
   std::chrono::steady_clock::time_point t0;
   rb_server_stats stats;
@@ -508,6 +543,30 @@ static int server_step(Server &S) {
     if (cls != RB_WF_GROUP) S.h_ctl[cls].total_tasks = (unsigned long long)tb;
   }
   for (int c = 1; c < RB_GROUPS; ++c) S.h_ctl[c].job_offset = jfirst[c];
+  // groups whose jobs share one scene and one setting run the uniform kernel
+  // (scene and settings as launch parameters); an empty group keeps what the
+  // graph has, so its capture stays valid
+  int uni_scene[RB_GROUPS];
+  Globals uni_G[RB_GROUPS];
+  for (int c = 0; c < RB_GROUPS; ++c) {
+    uni_scene[c] = S.graph_scene[c];
+    uni_G[c] = S.graph_G[c];
+  }
+  {
+    bool seen[RB_GROUPS] = {false};
+    for (size_t k = 0; k < plan.size(); ++k) {
+      const int cls = plan[k].cls;
+      if (cls == RB_WF_GROUP) continue;
+      const int sc = S.jobs[plan[k].id].req.scene;
+      if (!seen[cls]) {
+        seen[cls] = true;
+        uni_scene[cls] = sc;
+        uni_G[cls] = S.h_jobs[k].G;
+      } else if (uni_scene[cls] != sc || std::memcmp(&uni_G[cls], &S.h_jobs[k].G, sizeof(Globals)) != 0) {
+        uni_scene[cls] = -1;
+      }
+    }
+  }
   S.h_ctl[0].total_tasks = (unsigned long long)tb;             // all jobs (frames)
   S.h_ctl[0].njobs = (int)plan.size();
   const bool frames = S.o.frames_every > 0;
@@ -517,7 +576,13 @@ static int server_step(Server &S) {
   };
   auto launch_group = [&](int grp) {
     const int cls = grp > 4 ? grp - 4 : grp;
-    launch_batch(cls, minb_of(grp), grp > 4, S.st, S.d_jobs, S.d_ctl + grp, S.sms);
+    BatchUniform u;
+    const bool uniform = uni_scene[grp] >= 0;
+    if (uniform) {
+      u.S = S.scenes[uni_scene[grp]]->view;
+      u.G = uni_G[grp];
+    }
+    launch_batch(cls, minb_of(grp), grp > 4, S.st, S.d_jobs, S.d_ctl + grp, S.sms, uniform ? &u : nullptr);
   };
   auto kernels = [&](bool all_groups) {
     for (int c = 1; c < RB_GROUPS; ++c)
@@ -557,7 +622,11 @@ static int server_step(Server &S) {
     // from pinned staging when the graph runs, the three class kernels are
     // persistent (grid = resident blocks) and exit at once when their class
     // has no work this iteration.
-    if (!S.graph || S.graph_frames != (int)frames) {
+    bool same_uniform = true;
+    for (int c = 1; c < RB_GROUPS; ++c)
+      same_uniform = same_uniform && uni_scene[c] == S.graph_scene[c] &&
+                     std::memcmp(&uni_G[c], &S.graph_G[c], sizeof(Globals)) == 0;
+    if (!S.graph || S.graph_frames != (int)frames || !same_uniform) {
       if (S.graph) cudaGraphExecDestroy(S.graph);
       S.graph = nullptr;
       cudaGraph_t g;
@@ -570,6 +639,10 @@ static int server_step(Server &S) {
       if (!cuda_ok(cudaGraphInstantiate(&S.graph, g, 0), "graph instantiate")) return RB_ERR_CUDA;
       cudaGraphDestroy(g);
       S.graph_frames = (int)frames;
+      for (int c = 0; c < RB_GROUPS; ++c) {
+        S.graph_scene[c] = uni_scene[c];
+        S.graph_G[c] = uni_G[c];
+      }
     }
     cudaEventRecord(S.ev0, S.st);  // after any capture/instantiation: device time only
     if (!cuda_ok(cudaGraphLaunch(S.graph, S.st), "graph launch")) return RB_ERR_CUDA;
@@ -734,6 +807,10 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   }
   std::memset(S.h_jobs, 0, sizeof(BatchJob) * S.o.max_active_jobs);
   preload_batch_kernels();
+  for (int c = 0; c < RB_GROUPS; ++c) {
+    S.graph_scene[c] = -1;
+    std::memset(&S.graph_G[c], 0, sizeof(Globals));
+  }
   cudaEventCreate(&S.ev0);
   cudaEventCreate(&S.ev1);
   if (!cuda_ok(cudaStreamCreateWithFlags(&S.st_wf, cudaStreamNonBlocking), "server wavefront stream") ||
@@ -1036,7 +1113,11 @@ int rb_render_views(const rb_cuda_scene *scene, int n_views, int width, int heig
   const rb_render_opts o = current_opts();
   const int minb = o.reserved[0] > 0 ? std::min(o.reserved[0], 4) : batch_minb(ds->ms, G.nee != 0);
   BatchCtl *d_ctl = reinterpret_cast<BatchCtl *>(T.d);
-  launch_batch(ds->ms, minb, G.nee != 0, st, reinterpret_cast<const BatchJob *>(T.d + sizeof(BatchCtl)), d_ctl, sms);
+  BatchUniform uni;  // every view shares the scene and the settings
+  uni.S = ds->view;
+  uni.G = G;
+  launch_batch(ds->ms, minb, G.nee != 0, st, reinterpret_cast<const BatchJob *>(T.d + sizeof(BatchCtl)), d_ctl, sms,
+               &uni);
   if (!cuda_ok(cudaGetLastError(), "rb_render_views: launch")) return RB_ERR_CUDA;
   if (counters &&
       !cuda_ok(cudaMemcpyAsync(counters, &d_ctl->segments, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st),
