@@ -3,11 +3,12 @@
 // One persistent launch per iteration renders every active job: the
 // iteration's work is a list of pixel tasks (job, pixel, n samples) that warps
 // claim 32 at a time with one atomic per warp (ballot of the lanes that need
-// work). A lane runs its task's samples in the flattened segment loop of the
-// per-frame kernel and claims the next task the moment its pixel is done, so
-// lanes stay busy across task and job boundaries and one launch fills the GPU
-// whatever the jobs' sizes. A task owns its pixel for the launch, so the
-// pixel's sums are updated without atomics (Kahan in FP32, or FP64).
+// work). A lane traces its task's samples one whole path at a time (the
+// warp's camera rays start together, as in the per-frame kernel) and claims
+// the next task the moment its pixel is done, so lanes stay busy across task
+// and job boundaries and one launch fills the GPU whatever the jobs' sizes.
+// A task owns its pixel for the launch, so the pixel's sums are updated
+// without atomics (Kahan in FP32, or FP64).
 //
 // The serving loop (rb_server_*) keeps scenes resident, admits queued jobs as
 // slots and the HBM budget allow (continuous batching: new jobs join the next
@@ -171,14 +172,19 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
         }
       }
       if (alive) {
-        ++segs;
-        if (path_segment<NEE, MS>(job_or_uniform<UNI>(Su, J.S), job_or_uniform<UNI>(Gu, J.G), st, ovf, ray, thr, L,
-                                  bounce, prev_pdf, key, J.P.max_depth)) {
-          kahan_add(sx, cx, L.x);
-          kahan_add(sy, cy, L.y);
-          kahan_add(sz, cz, L.z);
-          alive = false;
+        // the whole path at once: a lane whose path ends early waits for the
+        // warp's longest, and the warp's next camera rays start together
+        // (coherent), as in the per-frame kernel's sample loop
+        bool end = false;
+        while (!end) {
+          ++segs;
+          end = path_segment<NEE, MS>(job_or_uniform<UNI>(Su, J.S), job_or_uniform<UNI>(Gu, J.G), st, ovf, ray, thr, L,
+                                      bounce, prev_pdf, key, J.P.max_depth);
         }
+        kahan_add(sx, cx, L.x);
+        kahan_add(sy, cy, L.y);
+        kahan_add(sz, cz, L.z);
+        alive = false;
       }
     }
   }
