@@ -118,8 +118,14 @@ __global__ void k_wf_fill(WfParams W, WfQueue q, int qi, int capacity) {
   }
 }
 
+// Four resident blocks per SM (64 registers): +7 % on the SDF field over
+// three at 72 (the traversal waits on its node loads). The shade kernel stays
+// at two (128 registers): three and four spill and ran 2-6 % slower.
+#ifndef WF_EXTEND_MINB
+#define WF_EXTEND_MINB 4
+#endif
 template <int MS>
-__global__ void __launch_bounds__(256) k_wf_extend(WfParams W, WfQueue q, int qi) {
+__global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(WfParams W, WfQueue q, int qi) {
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
