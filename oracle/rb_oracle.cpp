@@ -962,7 +962,7 @@ void orc_primary(void *sp, int w, int h, const double *fr, int32_t *ids, double 
         double t;
         const int id = trace(S, r, 0.001, 3.4028234663852886e38, t, false, c);
         ids[y * w + x] = id;
-        if (tout) tout[y * w + x] = id >= 0 ? t : -1.0;
+        if (tout) tout[y * w + x] = id != -1 ? t : -1.0;  // smooth-field hits (-2) report t too
       }
     nodes += c.nodes;
     prims += c.prims;

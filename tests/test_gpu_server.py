@@ -62,6 +62,37 @@ def test_same_alone_and_in_mix(cuda):
     mix.close()
 
 
+def test_shared_and_per_job_scene_kernels_agree(cuda):
+    """A class whose jobs share one scene and one setting runs the batched
+    kernel with the scene as a launch parameter; jobs of two scenes (or two
+    settings) in one class read it from the job table. Both give each job the
+    result it gets alone."""
+    spec = scenes.cornell(width=48, height=48)
+    sc = spec.to_scene()
+    sc.build_bvh()
+    ds_a, ds_b = sc.upload(), sc.upload()
+    fr = spec.camera.frame(48, 48)
+    mix = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=16)
+    ia, ib = mix.add_scene(ds_a), mix.add_scene(ds_b)
+    reqs = [serving.job(ia, fr, 48, 48, 32, spec.depth, background=0.0, seed=7),
+            serving.job(ib, fr, 48, 48, 32, spec.depth, background=0.0, seed=8),      # second scene: per-job records
+            serving.job(ia, fr, 48, 48, 32, spec.depth, background=0.0, light=2.0, seed=9)]  # other setting
+    jids = [mix.submit(r) for r in reqs]
+    mix.drain()
+    for r, jid, sid in zip(reqs, jids, (0, 1, 0)):
+        got = mix.fetch(jid, 48, 48)
+        alone = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=16)
+        aid = alone.add_scene(ds_a if sid == 0 else ds_b)
+        r.scene = aid
+        a = alone.submit(r)
+        alone.drain()
+        np.testing.assert_allclose(got, alone.fetch(a, 48, 48), rtol=RTOL, atol=ATOL_PER_SPP * 32)
+        alone.close()
+    mix.close()
+    ds_a.free()
+    ds_b.free()
+
+
 def test_server_matches_per_frame_kernel(cuda):
     spec = scenes.cornell(width=64, height=64)
     sc = spec.to_scene()
