@@ -594,7 +594,8 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     jobs/s over the one-weekend, Cornell, icosphere and SDF scenes, resolutions
     from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform [16, 1024], orbit
     angle U[0, 2pi). Plain = each job as its own per-frame launch, back to back;
-    served = the batched serving loop with real-time arrivals."""
+    served = the batched serving loop with real-time arrivals; backlog = the
+    same jobs all queued at once."""
     import torch
 
     from rayon_b200 import lib, render, scenes, serving
@@ -635,6 +636,18 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     wall = time.time() - tb
     st = srv.stats()
     srv.close()
+    # the same jobs as one backlog (all queued at once): the loop's throughput
+    # without the arrival ramp of the real-time trace
+    srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
+    ids = [srv.add_scene(ds) for ds in dss]
+    for r, j in zip(reqs, mix):
+        r.scene = ids[j["scene"]]
+        r.arrival_time = 0.0
+    tb = time.time()
+    srv.run_trace(reqs, realtime=False)
+    wall_backlog = time.time() - tb
+    st_backlog = srv.stats()
+    srv.close()
     for ds in dss:
         ds.free()
     return {"jobs": n_jobs, "arrival_rate_per_s": rate, "paths": paths,
@@ -642,6 +655,9 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
             "plain_per_job_mpaths_s": paths / plain / 1e6,
             "served_mpaths_s_wall": paths / wall / 1e6,
             "served_mpaths_s_device": st.paths / st.device_seconds / 1e6 if st.device_seconds else None,
+            "backlog_mpaths_s_device": (st_backlog.paths / st_backlog.device_seconds / 1e6
+                                        if st_backlog.device_seconds else None),
+            "backlog_mpaths_s_wall": paths / wall_backlog / 1e6,
             "p50_latency_s": st.p50_latency, "p99_latency_s": st.p99_latency, "mean_latency_s": st.mean_latency,
             "iterations": st.iterations, "peak_device_bytes": st.peak_device_bytes, "setup_s": setup,
             "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}

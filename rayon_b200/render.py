@@ -3,6 +3,7 @@ only); every kernel is the native library's."""
 from __future__ import annotations
 
 import ctypes as C
+import threading
 from contextlib import contextmanager
 
 import numpy as np
@@ -20,6 +21,25 @@ def _torch():
 def _stream_ptr():
     torch = _torch()
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+_staging = threading.local()
+
+
+def _pinned_like(t):
+    """A pinned host tensor of t's shape and dtype, kept per thread and reused:
+    the copy back runs at full DMA speed and touches no fresh pages."""
+    torch = _torch()
+    cache = getattr(_staging, "bufs", None)
+    if cache is None:
+        cache = _staging.bufs = {}
+    key = (tuple(t.shape), t.dtype)
+    buf = cache.get(key)
+    if buf is None:
+        if len(cache) > 8:
+            cache.clear()
+        buf = cache[key] = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    return buf
 
 
 def set_globals(light: float = 1.0, background: float = 1.0, fuzz: float = 0.8, glass_ior: float = 1.5,
@@ -99,10 +119,15 @@ def render_accumulate(ds, frame, w: int, h: int, spp: int, depth: int, backgroun
                                        C.c_void_p(buf[1].data_ptr()) if kahan else None,
                                        C.c_void_p(cnt.data_ptr()) if cnt is not None else None, _stream_ptr()),
               "rb_render_accumulate")
-        host = buf.cpu().numpy()  # synchronises the stream
-    img = host[0, :, :3].astype(np.float64)
-    if kahan:
-        img -= host[1, :, :3]  # Kahan: true sum = sum - compensation
+        stage = _pinned_like(buf)
+        stage.copy_(buf, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    host = stage.numpy()
+    img = np.empty((w * h, 3), np.float64)
+    if kahan:  # Kahan: true sum = sum - compensation, subtracted in FP64
+        np.subtract(host[0, :, :3], host[1, :, :3], out=img, dtype=np.float64)
+    else:
+        img[:] = host[0, :, :3]
     img = img.reshape(h, w, 3)
     set_globals()
     if counters:
