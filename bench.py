@@ -97,7 +97,7 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, keep: bool = False):
         import datetime
         if not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -110,7 +110,8 @@ class ClockSampler:
                 except ValueError:
                     continue
                 rows.append(p)
-        os.unlink(self.path)
+        if not keep:
+            os.unlink(self.path)
         window = "timed region"
         if self.t0 is not None and self.t1 is not None:
             inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
@@ -611,9 +612,13 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     mix = scenes.serving_mix(n_jobs, rate=rate, n_scenes=len(specs))
     frames = [scenes.orbit(specs[j["scene"]].camera, j["angle"]).frame(j["width"], j["height"]) for j in mix]
     paths = sum(j["width"] * j["height"] * j["spp"] for j in mix)
+    # clocks over each of the three runs (the section follows minutes of load)
+    clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))).__enter__()
+    clocks = {}
     # plain per-job launches
     torch.cuda.synchronize()
     tp = time.time()
+    clk.mark(True)
     for j, fr in zip(mix, frames):
         sp = specs[j["scene"]]
         render.set_globals(background=sp.background, dof=sp.dof)
@@ -625,6 +630,7 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
                                  None, None)
         torch.cuda.synchronize()
     plain = time.time() - tp
+    clk.mark(False)
     render.set_globals()
     srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
     ids = [srv.add_scene(ds) for ds in dss]
@@ -634,6 +640,7 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     tb = time.time()
     srv.run_trace(reqs, realtime=True)
     wall = time.time() - tb
+    clk_t = (tb, time.time())
     st = srv.stats()
     srv.close()
     # the same jobs as one backlog (all queued at once): the loop's throughput
@@ -646,8 +653,17 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     tb = time.time()
     srv.run_trace(reqs, realtime=False)
     wall_backlog = time.time() - tb
+    clk_b = (tb, time.time())
     st_backlog = srv.stats()
     srv.close()
+    clk.__exit__(None, None, None)
+    path_csv = clk.path
+    for name, (a, b) in (("plain", (clk.t0, clk.t1)), ("served", clk_t), ("backlog", clk_b)):
+        c = ClockSampler(clk.gpu)
+        c.path, c.t0, c.t1 = path_csv, a, b
+        clocks[name] = c.summary(keep=True)
+    if path_csv and os.path.exists(path_csv):
+        os.unlink(path_csv)
     for ds in dss:
         ds.free()
     return {"jobs": n_jobs, "arrival_rate_per_s": rate, "paths": paths,
@@ -660,6 +676,7 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
             "backlog_mpaths_s_wall": paths / wall_backlog / 1e6,
             "p50_latency_s": st.p50_latency, "p99_latency_s": st.p99_latency, "mean_latency_s": st.mean_latency,
             "iterations": st.iterations, "peak_device_bytes": st.peak_device_bytes, "setup_s": setup,
+            "clocks": clocks,
             "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}
 
 
