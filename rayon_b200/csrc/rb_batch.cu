@@ -338,6 +338,10 @@ struct Server {
   // marks the iteration's uploads, ev_wf the end of its wavefront runs
   cudaStream_t st_wf = nullptr;
   cudaEvent_t ev_up = nullptr, ev_wf = nullptr;
+  // job buffers come from a private stream-ordered pool that keeps freed
+  // memory (the device's default pool hands it back at every synchronisation,
+  // and mapping it again on the next admission stalls the loop)
+  cudaMemPool_t pool = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_frames = -1;
   // per class group: the scene shared by all its jobs (-1: none or several)
@@ -410,18 +414,18 @@ static bool admit(Server &S, Job &J) {
   const bool f64 = J.req.fp64_accum || J.req.spp > 65536 || on_wavefront(S, J);
   cudaError_t e;
   if (f64) {
-    e = cudaMallocAsync((void **)&J.acc64, n * 32, S.st);
+    e = cudaMallocFromPoolAsync((void **)&J.acc64, n * 32, S.pool, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.acc64, 0, n * 32, S.st);
   } else {
-    e = cudaMallocAsync((void **)&J.acc, n * 32, S.st);
+    e = cudaMallocFromPoolAsync((void **)&J.acc, n * 32, S.pool, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.acc, 0, n * 32, S.st);
   }
   if (e == cudaSuccess && frames) {
-    e = cudaMallocAsync((void **)&J.frame, n * 4, S.st);
+    e = cudaMallocFromPoolAsync((void **)&J.frame, n * 4, S.pool, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.frame, 0, n * 4, S.st);
   }
   if (e == cudaSuccess && J.req.converge_threshold > 0.0f) {
-    e = cudaMallocAsync((void **)&J.lum, n * 4, S.st);
+    e = cudaMallocFromPoolAsync((void **)&J.lum, n * 4, S.pool, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.lum, 0, n * 4, S.st);
   }
   if (e != cudaSuccess) {
@@ -819,6 +823,20 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
   }
   cudaEventCreate(&S.ev0);
   cudaEventCreate(&S.ev1);
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (!cuda_ok(cudaMemPoolCreate(&S.pool, &props), "server job pool")) {
+      S.pool = nullptr;
+      rb_server_destroy(r);
+      return nullptr;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(S.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (!cuda_ok(cudaStreamCreateWithFlags(&S.st_wf, cudaStreamNonBlocking), "server wavefront stream") ||
       !cuda_ok(cudaEventCreateWithFlags(&S.ev_up, cudaEventDisableTiming), "server event") ||
       !cuda_ok(cudaEventCreateWithFlags(&S.ev_wf, cudaEventDisableTiming), "server event")) {
@@ -852,6 +870,10 @@ void rb_server_destroy(rb_server *r) {
   }
   if (S.ev_up) cudaEventDestroy(S.ev_up);
   if (S.ev_wf) cudaEventDestroy(S.ev_wf);
+  if (S.pool) {
+    if (S.st) cudaStreamSynchronize(S.st);  // the jobs' stream-ordered frees have run
+    cudaMemPoolDestroy(S.pool);
+  }
   if (S.own_stream && S.st) cudaStreamDestroy(S.st);
   delete r;
 }

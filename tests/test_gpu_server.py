@@ -208,6 +208,43 @@ def test_sdf_field_jobs_on_the_wavefront_engine(cuda):
     ds.free()
 
 
+def test_wavefront_jobs_beside_class_kernels(cuda):
+    # an iteration with smooth-SDF jobs runs them on the wavefront engine's
+    # stream while the class kernels run; every job still gets its alone result
+    sdf = scenes.sdf_field(count=48, width=48, height=32)
+    box = scenes.cornell(width=64, height=64)
+    dss = []
+    for spec in (sdf, box):
+        sc = spec.to_scene()
+        sc.build_bvh()
+        dss.append(sc.upload())
+    reqs = [(0, 48, 32, 16), (1, 64, 64, 32), (0, 40, 24, 8), (1, 48, 48, 16)]
+    specs = (sdf, box)
+
+    def job(ids, k, si, w, h, spp):
+        sp = specs[si]
+        return serving.job(ids[si], sp.camera.frame(w, h), w, h, spp, sp.depth, background=sp.background,
+                           seed=50 + k)
+
+    mix = serving.Server(paths_per_iteration=1 << 16, max_spp_per_iteration=8)
+    ids = [mix.add_scene(ds) for ds in dss]
+    jids = [mix.submit(job(ids, k, *r)) for k, r in enumerate(reqs)]
+    mix.drain()
+    for k, (r, jid) in enumerate(zip(reqs, jids)):
+        si, w, h, spp = r
+        assert mix.status(jid).spp_done == spp
+        got = mix.fetch(jid, w, h)
+        alone = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=64)
+        aid = [alone.add_scene(ds) for ds in dss]
+        a = alone.submit(job(aid, k, *r))
+        alone.drain()
+        np.testing.assert_allclose(got, alone.fetch(a, w, h), rtol=RTOL, atol=ATOL_PER_SPP * spp)
+        alone.close()
+    mix.close()
+    for ds in dss:
+        ds.free()
+
+
 def test_latency_target_controller(cuda):
     # the path quantum follows clamp(target / measured, 0.5, 2) per full
     # iteration: from a 64 M-path quantum it settles where an iteration takes
