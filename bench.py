@@ -296,6 +296,9 @@ WORKLOADS = {
 # engine per workload: the per-pixel / batched kernel, or the wavefront engine
 # (whose separate field-march kernel is the faster one for SDF fields)
 ENGINE = {"sdf_field": "wavefront"}
+# wavefront queue: 16 M path slots (about 10 GB with the SDF march buffers);
+# 4 M -> 8 M -> 16 M measured 513 -> 537 -> 545 Mpaths/s on the SDF field
+WF_QUEUE = 1 << 24
 
 
 def workload_spec(name: str, small: bool = False):
@@ -371,7 +374,7 @@ def main():
         cp = C.c_void_p(cnt.data_ptr()) if cnt is not None else None
         if engine == "wavefront":
             st = lib.rb_render_views_wavefront(ds.handle, nviews, w, h, frp, spp, base, depth,
-                                               C.c_void_p(acc.data_ptr()), 1 << 22, cp, sptr)
+                                               C.c_void_p(acc.data_ptr()), WF_QUEUE, cp, sptr)
         elif nviews > 1:
             st = lib.rb_render_views(ds.handle, nviews, w, h, frp, spp, base, depth, C.c_void_p(acc.data_ptr()),
                                      cp, sptr)
@@ -440,7 +443,7 @@ def main():
                 d2h = 5 * npx * 12
             elif engine == "wavefront":
                 img = render.render_views_wavefront(ds2, list(frames), w, h, spp, depth, background=spec.background,
-                                                    dof=spec.dof, queue_capacity=1 << 22)
+                                                    dof=spec.dof, queue_capacity=WF_QUEUE)
                 h2d = ds2.nbytes + frames.nbytes
                 d2h = nviews * npx * 32
             elif nviews > 1:
