@@ -404,11 +404,11 @@ __global__ void k_job_converge(const float4 *__restrict__ acc, const double *__r
 // SDF march buffers, held for the process beside the jobs' HBM budget);
 // 4 M -> 8 M measured +4.6 % on the SDF field.
 #define RB_SERVER_WF_QUEUE (1 << 23)
-static bool on_wavefront(const Server &S, const Job &J) {
-  if (!S.o.wavefront_field) return false;
-  const rbd::SceneView &v = S.scenes[J.req.scene]->view;
-  return S.scenes[J.req.scene]->ms >= RB_MS_SDF && v.sdf_k > 0.0f && v.num_sdf > 0;
+static bool on_wavefront_scene(const Server &S, const DeviceScene *ds) {
+  return S.o.wavefront_field && ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0;
 }
+
+static bool on_wavefront(const Server &S, const Job &J) { return on_wavefront_scene(S, S.scenes[J.req.scene]); }
 
 static bool admit(Server &S, Job &J) {
   const bool frames = S.o.frames_every > 0;
@@ -888,6 +888,12 @@ int rb_server_add_scene(rb_server *r, const rb_cuda_scene *scene) {
   if (!ds) {
     set_error("rb_server_add_scene: unknown scene handle");
     return RB_ERR_NOT_FOUND;
+  }
+  // the wavefront engine's queues and march buffers are allocated when a
+  // smooth-SDF scene joins, not inside the first request's iteration
+  if (on_wavefront_scene(r->s, ds)) {
+    const int rc = wf_render_jobs(ds, nullptr, 0, RB_SERVER_WF_QUEUE, nullptr, r->s.st);
+    if (rc != RB_OK) return rc;
   }
   r->s.scenes.push_back(ds);
   return (int)r->s.scenes.size() - 1;

@@ -746,7 +746,9 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
     total += (unsigned long long)jobs[j].P.width * jobs[j].P.height * (unsigned long long)jobs[j].P.samples;
     nee = nee || jobs[j].G.nee != 0;
   }
-  if (total == 0) return RB_OK;
+  const bool field = ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0;
+  if (field && !wf_alloc_march(E)) return RB_ERR_OUT_OF_MEMORY;
+  if (total == 0) return RB_OK;  // (a call without work only allocates)
   std::memcpy(E.h_jobs, jobs, sizeof(WfJob) * njobs);
   WfParams W;
   std::memset(&W, 0, sizeof W);
@@ -754,8 +756,7 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
   W.jobs = E.d_jobs;
   W.njobs = njobs;
   W.ctl = E.ctl;
-  if (ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0) {
-    if (!wf_alloc_march(E)) return RB_ERR_OUT_OF_MEMORY;
+  if (field) {
     W.cand = E.cand;
     W.ncand = E.ncand;
     W.list = E.list;
