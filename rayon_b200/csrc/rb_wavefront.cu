@@ -192,18 +192,34 @@ __device__ __forceinline__ int4 wf_cand(const WfParams &W, const int4 (&cr)[WF_C
 // in index order, its candidates whose window holds t (and the next window
 // entry beyond t); then the lanes fold their k-th marked candidate at the
 // same time, k = 0, 1, ... (the fold order per lane is still index order).
-__device__ __forceinline__ float wf_field(const SceneView &S, const WfParams &W, const float4 *tab, int slot, int n,
-                                          const int4 (&cr)[WF_CAND_REG], const f3 &p, float t, float &next,
-                                          int *nearest, int &lone) {
-  uint32_t active = 0;
-  float nx = RB_SDF_FAR;
+//
+// The mark pass: the candidates whose window holds t, the next entry beyond
+// t, and the earliest exit among the held windows. The set stays the same
+// while t < next and t <= that exit (t never decreases along a march), so the
+// march recomputes it only when t leaves that range.
+__device__ __forceinline__ void wf_mark(const WfParams &W, const int4 (&cr)[WF_CAND_REG], int slot, int n, float t,
+                                        uint32_t &active, float &next, float &exit) {
+  uint32_t a = 0;
+  float nx = RB_SDF_FAR, ex = RB_SDF_FAR;
   for (int i = 0; i < n; ++i) {
     const int4 e = wf_cand(W, cr, slot, i);
-    const float t0 = __int_as_float(e.y);
+    const float t0 = __int_as_float(e.y), t1 = __int_as_float(e.z);
     if (t0 > t) nx = fminf(nx, t0);
-    else if (t <= __int_as_float(e.z)) active |= 1u << i;
+    else if (t <= t1) {
+      a |= 1u << i;
+      ex = fminf(ex, t1);
+    }
   }
+  active = a;
   next = nx;
+  exit = ex;
+}
+
+// The fold pass over the marked candidates: the field at p (RB_SDF_FAR when
+// none is marked); `lone` is the candidate code when exactly one is marked.
+__device__ __forceinline__ float wf_fold(const SceneView &S, const WfParams &W, const float4 *tab, int slot,
+                                         const int4 (&cr)[WF_CAND_REG], uint32_t active, const f3 &p, int *nearest,
+                                         int &lone) {
   const bool single = active != 0u && (active & (active - 1u)) == 0u;
   lone = -1;
   float F = RB_SDF_FAR, best = RB_SDF_FAR;
@@ -262,6 +278,9 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
   const float e = RB_SDF_NORMAL_EPS;
   int slot = 0, n = 0, steps = 0, phase = WF_ESCAPE, sub = 0, nearest = 0, prev = -1;
   float prev_d = 0.f;
+  // the lane's marked window set and the t range it holds for (wf_mark)
+  uint32_t marked = 0;
+  float mark_next = -1.f, mark_exit = -1.f;
   int4 cr[WF_CAND_REG];
 #pragma unroll
   for (int i = 0; i < WF_CAND_REG; ++i) cr[i] = make_int4(0, 0, 0, 0);
@@ -297,6 +316,7 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
           sub = 0;
           steps = 0;
           prev = -1;
+          mark_next = -1.f;  // mark again for the new ray
           busy = true;
         } else {
           drained = true;
@@ -314,9 +334,10 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
     } else {
       pe = r.at(t);
     }
-    float next;
+    if (!(t < mark_next && t <= mark_exit)) wf_mark(W, cr, slot, n, t, marked, mark_next, mark_exit);
+    const float next = mark_next;
     int near = cr[0].x >> 1, lone;
-    const float raw = wf_field(S, W, tab, slot, n, cr, pe, t, next, phase == WF_NORMAL ? nullptr : &near, lone);
+    const float raw = wf_fold(S, W, tab, slot, cr, marked, pe, phase == WF_NORMAL ? nullptr : &near, lone);
     bool finished = false;
     if (phase == WF_NORMAL) {
       if (sub & 1) {
