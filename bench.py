@@ -167,6 +167,26 @@ def profiled_issue_active():
     return None
 
 
+def profiled_figures(name: str) -> dict:
+    """The `key: value` lines (unindented) of a committed ncu summary under
+    profiles/, numbers as floats."""
+    out = {}
+    f = ROOT / "profiles" / name
+    if not f.exists():
+        return out
+    for line in f.read_text().splitlines():
+        if not line or line[0].isspace() or ":" not in line:
+            continue
+        k, v = (s.strip() for s in line.split(":", 1))
+        if not v:
+            continue
+        try:
+            out[k] = float(v)
+        except ValueError:
+            out[k] = v
+    return out
+
+
 def _port_sample(spec, cam, budget_s: float):
     """The FP64 oracle (this project's CPU restatement of the path, all host
     threads) on a seeded subset of the frame's pixels at full spp, scaled to
@@ -516,6 +536,16 @@ def main():
         # the kernel is bound by instruction issue, not HBM: its issue-slot
         # utilisation from the committed ncu capture of the same launch
         res["roofline"]["issue_active_frac_ncu"] = profiled_issue_active()
+    if args.workload == "icospheres":
+        # 252 MB of scene, twice L2: traversal is bound by load latency, not
+        # bandwidth; the achieved L2 / DRAM rates and issue utilisation come from
+        # the committed ncu capture of this kernel on this frame
+        fig = profiled_figures("k_render_icospheres.txt")
+        for k in ("l2_gbs_ncu", "dram_gbs_ncu", "issue_active_frac_ncu", "ncu_case"):
+            if k in fig:
+                res["roofline"][k] = fig[k]
+        if "dram_gbs_ncu" in fig:
+            res["roofline"]["dram_frac_ncu"] = fig["dram_gbs_ncu"] / peaks["hbm_gbs"]
     if args.workload == "icospheres" and not args.small:
         # the configuration asks for 8-bit quantised child bounds vs FP32 nodes
         res["quantized_bvh"] = quantized_compare(sc, fr, w, h, spp, depth, step_ms=t_ms)
