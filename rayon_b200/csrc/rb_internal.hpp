@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/rayon_b200.h"
@@ -28,11 +30,31 @@ inline uint32_t __float_as_uint_host(float f) {
   return i;
 }
 
+// Allocator that leaves elements uninitialised on a value-less resize, so a
+// large host array is first touched (and its pages faulted in) by the threads
+// that fill it rather than by one thread zeroing it.
+template <class T>
+struct uninit_alloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = uninit_alloc<U>;
+  };
+  uninit_alloc() = default;
+  template <class U>
+  uninit_alloc(const uninit_alloc<U> &) noexcept {}
+  template <class U>
+  void construct(U *) noexcept {}
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new ((void *)p) U(std::forward<A>(a)...);
+  }
+};
+
 // Device layout assembled on the host before upload.
 struct HostLayout {
-  std::vector<float4> nodes;          // 4 per interior node
+  std::vector<float4, uninit_alloc<float4>> nodes;  // 4 per interior node, every word written
   std::vector<rbd::QNode> qnodes;     // quantised copy of nodes
-  std::vector<float4> prims;          // 3 per primitive
+  std::vector<float4, uninit_alloc<float4>> prims;  // 3 per primitive, zeroed record by record
   std::vector<float4> normals;        // 3 per primitive (vertex normals) or empty
   std::vector<rbd::DevMaterial> mats;
   std::vector<rbd::LightRec> lights;

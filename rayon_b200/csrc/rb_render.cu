@@ -142,11 +142,26 @@ static void parallel_chunks(size_t n, F fn) {
 
 static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts, HostLayout &L) {
   const size_t n = hs.geoms.size();
-  L.prims.assign(3 * n, make_float4(0, 0, 0, 0));
+  L.prims.resize(3 * n);  // uninitialised: each record is zeroed by the thread that converts it
   L.mats.resize(hs.materials.size());
   for (size_t i = 0; i < hs.materials.size(); ++i) L.mats[i] = resolve_material(hs.materials[i]);
-  bool any_normals = false;
-  for (const auto &g : hs.geoms) any_normals |= (g.type == RB_GEOM_TRIANGLE && g.has_normals);
+  // scene-wide flags in one parallel pass over the geometries
+  std::atomic<bool> f_normals{false}, f_sdf{false}, f_displaced{false};
+  parallel_chunks(n, [&](size_t b, size_t e) {
+    bool nrm = false, sdf = false, disp = false;
+    for (size_t i = b; i < e; ++i) {
+      const Geom &g = hs.geoms[i];
+      nrm |= (g.type == RB_GEOM_TRIANGLE && g.has_normals);
+      sdf |= g.type == RB_GEOM_SDF_PRIMITIVE;
+      disp |= g.type == RB_GEOM_DISPLACED_SPHERE;
+    }
+    if (nrm) f_normals.store(true, std::memory_order_relaxed);
+    if (sdf) f_sdf.store(true, std::memory_order_relaxed);
+    if (disp) f_displaced.store(true, std::memory_order_relaxed);
+  });
+  const bool any_normals = f_normals.load(), any_sdf = f_sdf.load(), any_displaced = f_displaced.load();
+  bool any_light_mat = false;
+  for (const auto &m : L.mats) any_light_mat |= m.kind == L_LIGHT;
   if (any_normals) L.normals.assign(3 * n, make_float4(0, 0, 0, 0));
   L.sdf.clear();
   double light_area = 0.0;
@@ -162,6 +177,7 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     for (size_t i = b; i < e; ++i) {
       const Geom &g = hs.geoms[i];
       float4 *r = &L.prims[3 * i];
+      std::memset(r, 0, 3 * sizeof(float4));
       uint32_t kind = PK_NONE;
       switch (g.type) {
         case RB_GEOM_SPHERE:
@@ -197,7 +213,9 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
       put(r, 11, __uint_as_float_host(tag_of(g, kind)));
     }
   });
-  for (size_t i = 0; i < n; ++i) {
+  // SDF table and emitters, in geometry order; only scenes that hold either need the pass
+  const size_t n_walk = (any_sdf || any_light_mat) ? n : 0;
+  for (size_t i = 0; i < n_walk; ++i) {
     const Geom &g = hs.geoms[i];
     float4 *r = &L.prims[3 * i];
     uint32_t kind = tag_kind(__float_as_uint_host(getw(r, 11)));
@@ -265,10 +283,8 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     if (m.kind == L_MIRROR || m.kind == L_ROUGH_MIRROR || m.kind == L_GLASS) L.ms = std::max(L.ms, RB_MS_CLASSIC);
     if (m.kind == L_ANISO_METAL || m.kind == L_THIN_FILM || m.kind == L_CLEAR_COAT || m.pattern) L.ms = RB_MS_FULL;
   }
-  for (const auto &g : hs.geoms) {
-    if (g.type == RB_GEOM_DISPLACED_SPHERE) L.ms = std::max(L.ms, RB_MS_FULL);
-    if (g.type == RB_GEOM_SDF_PRIMITIVE) L.ms = RB_MS_SDF;
-  }
+  if (any_displaced) L.ms = std::max(L.ms, RB_MS_FULL);
+  if (any_sdf) L.ms = RB_MS_SDF;
   if (!L.lights.empty()) L.lights.back().cdf = 3.0e38f;  // the last bin takes any rounding excess
 
   // BVH: interior nodes only, each holding its two children's boxes.
@@ -292,7 +308,7 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
         return false;
       }
     // interior node i goes to slot remap[i]: independent writes, in parallel
-    L.nodes.assign(4 * (size_t)m, make_float4(0, 0, 0, 0));
+    L.nodes.resize(4 * (size_t)m);  // uninitialised: the loop below writes every word of every slot
     parallel_chunks(hs.nodes.size(), [&](size_t b, size_t e) {
       for (size_t i = b; i < e; ++i) {
         const Node &nd = hs.nodes[i];
@@ -362,8 +378,8 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
   return true;
 }
 
-template <typename T>
-static bool upload_vec(const std::vector<T> &v, T **dst, cudaStream_t st, size_t &bytes) {
+template <typename T, typename A>
+static bool upload_vec(const std::vector<T, A> &v, T **dst, cudaStream_t st, size_t &bytes) {
   *dst = nullptr;
   if (v.empty()) return true;
   const size_t nb = v.size() * sizeof(T);
