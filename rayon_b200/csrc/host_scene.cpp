@@ -146,6 +146,7 @@ struct Builder {
   const std::vector<Geom> &g;
   std::vector<int> idx;                  // geometry order, permuted in place
   std::vector<double> cent[3];           // centroid per axis, (bmin + bmax) * 0.5
+  std::vector<double> box;               // 6 per geometry: bmin xyz, bmax xyz (compact copy)
   int max_leaf;
 
   explicit Builder(const std::vector<Geom> &geoms, int ml) : g(geoms), max_leaf(ml) {
@@ -153,13 +154,21 @@ struct Builder {
     idx.resize(n);
     for (size_t i = 0; i < n; ++i) idx[i] = (int)i;
     for (int a = 0; a < 3; ++a) cent[a].resize(n);
+    box.resize(6 * n);
     for (size_t i = 0; i < n; ++i) {
       const V3 c = (g[i].bmin + g[i].bmax) * 0.5;
       cent[0][i] = c.x; cent[1][i] = c.y; cent[2][i] = c.z;
+      double *b = &box[6 * i];
+      b[0] = g[i].bmin.x; b[1] = g[i].bmin.y; b[2] = g[i].bmin.z;
+      b[3] = g[i].bmax.x; b[4] = g[i].bmax.y; b[5] = g[i].bmax.z;
     }
   }
 
-  void sort_axis(int start, int end, int axis, std::vector<std::pair<double, int>> &buf) {
+  // Sorts idx[start, end) by centroid on `axis`; when sorted_boxes is given,
+  // also writes the boxes of the range in the new order (6 doubles each), so
+  // that the SAH sweeps read them sequentially.
+  void sort_axis(int start, int end, int axis, std::vector<std::pair<double, int>> &buf,
+                 std::vector<double> *sorted_boxes = nullptr) {
     const int n = end - start;
     buf.resize(n);
     const double *key = cent[axis].data();
@@ -169,6 +178,11 @@ struct Builder {
                 return a.first < b.first;
               });
     for (int i = 0; i < n; ++i) idx[start + i] = buf[i].second;
+    if (sorted_boxes) {
+      sorted_boxes->resize(6 * (size_t)n);
+      double *o = sorted_boxes->data();
+      for (int i = 0; i < n; ++i) std::memcpy(o + 6 * (size_t)i, &box[6 * (size_t)buf[i].second], 6 * sizeof(double));
+    }
   }
 
   static float area_f(double ex, double ey, double ez) {
@@ -181,9 +195,9 @@ struct Builder {
   int split(int start, int end, Node &node) {
     double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
     for (int i = start; i < end; ++i) {
-      const Geom &q = g[idx[i]];
-      lo[0] = std::min(lo[0], q.bmin.x); lo[1] = std::min(lo[1], q.bmin.y); lo[2] = std::min(lo[2], q.bmin.z);
-      hi[0] = std::max(hi[0], q.bmax.x); hi[1] = std::max(hi[1], q.bmax.y); hi[2] = std::max(hi[2], q.bmax.z);
+      const double *q = &box[6 * (size_t)idx[i]];
+      lo[0] = std::min(lo[0], q[0]); lo[1] = std::min(lo[1], q[1]); lo[2] = std::min(lo[2], q[2]);
+      hi[0] = std::max(hi[0], q[3]); hi[1] = std::max(hi[1], q[4]); hi[2] = std::max(hi[2], q[5]);
     }
     for (int a = 0; a < 3; ++a) { node.bmin[a] = lo[a]; node.bmax[a] = hi[a]; }
     const int count = end - start;
@@ -199,26 +213,27 @@ struct Builder {
     const float parent_area = area_f(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
 
     thread_local std::vector<std::pair<double, int>> buf;
+    thread_local std::vector<double> sb;  // the range's boxes in sorted order, 6 per entry
     thread_local std::vector<double> pmin, pmax, smin, smax;  // 3 per entry
     pmin.resize(3 * (size_t)count); pmax.resize(3 * (size_t)count);
     smin.resize(3 * (size_t)count); smax.resize(3 * (size_t)count);
 
     for (int axis = 0; axis < 3; ++axis) {
-      sort_axis(start, end, axis, buf);
+      sort_axis(start, end, axis, buf, &sb);
       double rl[3] = {1e30, 1e30, 1e30}, rh[3] = {-1e30, -1e30, -1e30};
       for (int i = 0; i < count; ++i) {
-        const Geom &q = g[idx[start + i]];
-        rl[0] = std::min(rl[0], q.bmin.x); rl[1] = std::min(rl[1], q.bmin.y); rl[2] = std::min(rl[2], q.bmin.z);
-        rh[0] = std::max(rh[0], q.bmax.x); rh[1] = std::max(rh[1], q.bmax.y); rh[2] = std::max(rh[2], q.bmax.z);
+        const double *q = &sb[6 * (size_t)i];
+        rl[0] = std::min(rl[0], q[0]); rl[1] = std::min(rl[1], q[1]); rl[2] = std::min(rl[2], q[2]);
+        rh[0] = std::max(rh[0], q[3]); rh[1] = std::max(rh[1], q[4]); rh[2] = std::max(rh[2], q[5]);
         std::memcpy(&pmin[3 * i], rl, sizeof rl);
         std::memcpy(&pmax[3 * i], rh, sizeof rh);
       }
       rl[0] = rl[1] = rl[2] = 1e30;
       rh[0] = rh[1] = rh[2] = -1e30;
       for (int i = count - 1; i >= 0; --i) {
-        const Geom &q = g[idx[start + i]];
-        rl[0] = std::min(rl[0], q.bmin.x); rl[1] = std::min(rl[1], q.bmin.y); rl[2] = std::min(rl[2], q.bmin.z);
-        rh[0] = std::max(rh[0], q.bmax.x); rh[1] = std::max(rh[1], q.bmax.y); rh[2] = std::max(rh[2], q.bmax.z);
+        const double *q = &sb[6 * (size_t)i];
+        rl[0] = std::min(rl[0], q[0]); rl[1] = std::min(rl[1], q[1]); rl[2] = std::min(rl[2], q[2]);
+        rh[0] = std::max(rh[0], q[3]); rh[1] = std::max(rh[1], q[4]); rh[2] = std::max(rh[2], q[5]);
         std::memcpy(&smin[3 * i], rl, sizeof rl);
         std::memcpy(&smax[3 * i], rh, sizeof rh);
       }
