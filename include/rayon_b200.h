@@ -117,8 +117,10 @@ void convertAccumToDisplayCUDA(void *d_accum_buffer, unsigned char *display_imag
  * that is part of the library (held on every GPU that loads it until exit):
  * width * height * channels above 8388608 is rejected with RB_ERR_CAPACITY.
  * Allocates nothing. The array's device address is looked up on the first call
- * per device (make that call before any stream capture). Calls share the array,
- * so calls that overlap on the GPU race. Returns an rb_status. */
+ * per device (make that call before any stream capture) and cached; the cache
+ * does not survive cudaDeviceReset. Calls share the array, so calls that
+ * overlap on the GPU race. The kernel and the copy run on the legacy default
+ * stream. Returns an rb_status. */
 int convertAccumToDisplayNoAlloc(void *d_accum_buffer, unsigned char *display_image, int width,
                                  int height, int channels, int num_samples, float gamma,
                                  void *d_pixel_sample_counts);

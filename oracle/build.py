@@ -10,7 +10,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_build" / "liboracle.so"
-REFERENCE = Path("/root/reference")
+# The reference tree the drivers compile from: RAYON_REFERENCE, by default the
+# read-only checkout at /root/reference.
+REFERENCE = Path(os.environ.get("RAYON_REFERENCE", "/root/reference"))
 
 
 def build_oracle(verbose: bool = False) -> Path:

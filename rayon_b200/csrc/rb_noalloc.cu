@@ -19,6 +19,13 @@
 // keeps the previous call's bytes; the kernel writes every byte the call
 // copies out, so nothing needs clearing. Calls that overlap on the GPU (from
 // different host threads or streams) race on the array.
+//
+// The conversion kernel and the copy out run on the legacy default stream, as
+// convertAccumToDisplayCUDA's callers expect: a caller that writes the
+// accumulation from a non-blocking stream orders those writes before the call.
+// The cached address does not survive cudaDeviceReset (the reset unloads the
+// module that holds the array): a process that resets a device does not call
+// this entry point on it again.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -39,12 +46,12 @@ static unsigned char *g_scratch_addr[RB_NOALLOC_MAX_DEVICES] = {nullptr};
 
 // Same per-pixel arithmetic as the display kernel of convertAccumToDisplayCUDA
 // (gammaCorrectKernel, render_acc_kernel.cu:11-44).
-__global__ void k_gamma_static(const float4 *__restrict__ acc, unsigned char *__restrict__ out, int w, int h, int spp,
+// One thread per pixel on a 1-D grid, so any image that fits the array
+// (a 1 x 2,796,202 RGB strip included) stays within the launch limits.
+__global__ void k_gamma_static(const float4 *__restrict__ acc, unsigned char *__restrict__ out, int npix, int spp,
                                int ch, float gamma, const int *__restrict__ counts) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const int pix = y * w + x;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= npix) return;
   const float4 a = acc[pix];
   int n = counts ? abs(counts[pix]) : spp;
   if (n <= 0) n = 1;
@@ -95,9 +102,10 @@ extern "C" int convertAccumToDisplayNoAlloc(void *d_accum_buffer, unsigned char 
     }
     scratch = g_scratch_addr[dev];
   }
-  dim3 blk(32, 8), grd((width + 31) / 32, (height + 7) / 8);
-  k_gamma_static<<<grd, blk>>>(static_cast<const float4 *>(d_accum_buffer), scratch, width, height, num_samples,
-                               channels, gamma, static_cast<const int *>(d_pixel_sample_counts));
+  // bytes <= 8 MiB and channels >= 3 bound the pixel count well inside int
+  const int npix = width * height;
+  k_gamma_static<<<(npix + 255) / 256, 256>>>(static_cast<const float4 *>(d_accum_buffer), scratch, npix, num_samples,
+                                               channels, gamma, static_cast<const int *>(d_pixel_sample_counts));
   g_launches++;
   if (!cuda_ok(cudaGetLastError(), "convertAccumToDisplayNoAlloc: launch")) return RB_ERR_CUDA;
   if (!cuda_ok(cudaMemcpy(display_image, scratch, bytes, cudaMemcpyDeviceToHost),

@@ -622,12 +622,11 @@ __global__ void k_fold_slices(float4 *__restrict__ acc, float4 *__restrict__ com
 }
 
 // accum float4 sums -> u8 (gammaCorrectKernel, render_acc_kernel.cu:11-44)
-__global__ void k_gamma(const float4 *__restrict__ acc, unsigned char *__restrict__ out, int w, int h, int spp,
-                        int ch, float gamma, const int *__restrict__ counts) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const int pix = y * w + x;
+// (one thread per pixel on a 1-D grid: no grid.y limit on tall images)
+__global__ void k_gamma(const float4 *__restrict__ acc, unsigned char *__restrict__ out, int npix, int spp, int ch,
+                        float gamma, const int *__restrict__ counts) {
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= npix) return;
   const float4 a = acc[pix];
   int n = counts ? abs(counts[pix]) : spp;
   if (n <= 0) n = 1;
@@ -649,12 +648,10 @@ __constant__ float c_plasma[8][4] = {
     {0.429f, 0.650f, 0.060f, 0.540f}, {0.571f, 0.820f, 0.170f, 0.360f}, {0.714f, 0.940f, 0.340f, 0.170f},
     {0.857f, 0.990f, 0.560f, 0.040f}, {1.000f, 0.940f, 0.975f, 0.130f}};
 
-__global__ void k_heatmap(const int *__restrict__ counts, unsigned char *__restrict__ out, int w, int h, int ch,
+__global__ void k_heatmap(const int *__restrict__ counts, unsigned char *__restrict__ out, int npix, int ch,
                           int max_s) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const int pix = y * w + x;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= npix) return;
   const int c = abs(counts[pix]);
   float t = max_s > 0 ? fminf((float)c / (float)max_s, 1.0f) : 0.0f;
   t = fminf(fmaxf(t, 0.0f), 1.0f);
@@ -1282,13 +1279,13 @@ unsigned long long renderPixelsCUDAAccumulative(
 
 void convertAccumToDisplayCUDA(void *d_acc, unsigned char *img, int w, int h, int ch, int spp, float gamma,
                                void *counts) {
-  if (!d_acc || !img || spp <= 0) return;
+  if (!d_acc || !img || spp <= 0 || w <= 0 || h <= 0 || (int64_t)w * h > INT32_MAX) return;
   const size_t bytes = (size_t)w * h * ch;
   if (!ensure_display(bytes)) return;
-  dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
+  const int npix = w * h;
   cudaStream_t st = s_display ? s_display : 0;
-  k_gamma<<<grd, blk, 0, st>>>(static_cast<const float4 *>(d_acc), s_dev_display, w, h, spp, ch, gamma,
-                                static_cast<const int *>(counts));
+  k_gamma<<<(npix + 255) / 256, 256, 0, st>>>(static_cast<const float4 *>(d_acc), s_dev_display, npix, spp, ch, gamma,
+                                               static_cast<const int *>(counts));
   g_launches++;
   finish_display(img, bytes);
 }
@@ -1319,12 +1316,12 @@ int countConvergedPixels(void *p, int n) {
 }
 
 void renderSampleHeatmapCUDA(void *counts, unsigned char *img, int w, int h, int ch, int max_s) {
-  if (!counts || !img) return;
+  if (!counts || !img || w <= 0 || h <= 0 || (int64_t)w * h > INT32_MAX) return;
   const size_t bytes = (size_t)w * h * ch;
   if (!ensure_display(bytes)) return;
-  dim3 blk(32, 8), grd((w + 31) / 32, (h + 7) / 8);
-  k_heatmap<<<grd, blk, 0, s_display ? s_display : 0>>>(static_cast<const int *>(counts), s_dev_display, w, h, ch,
-                                                          max_s);
+  const int npix = w * h;
+  k_heatmap<<<(npix + 255) / 256, 256, 0, s_display ? s_display : 0>>>(static_cast<const int *>(counts), s_dev_display,
+                                                                       npix, ch, max_s);
   g_launches++;
   finish_display(img, bytes);
 }

@@ -1,6 +1,8 @@
 """convertAccumToDisplayNoAlloc: the allocation-free display conversion gives the
 same image as convertAccumToDisplayCUDA, on two calls in a row that share its
-fixed staging array, and refuses images larger than that array.
+fixed staging array, with and without per-pixel sample counts, for a strip
+taller than a 2-D launch grid could cover; it leaves the device's free memory
+unchanged and refuses images larger than that array.
 
 It exists for callers that cannot allocate device memory when they want a
 frame: device memory owned by another allocator or held to a fixed budget,
@@ -26,15 +28,16 @@ def _frame_accum(ds, spec, w, h, spp, rng, dacc):
     assert n == w * h * spp
 
 
-def _existing(dacc, w, h, ch, spp, gamma=2.0):
+def _existing(dacc, w, h, ch, spp, gamma=2.0, counts=None):
     out = np.zeros(w * h * ch, np.uint8)
-    lib.convertAccumToDisplayCUDA(dacc, out.ctypes.data_as(C.POINTER(C.c_uint8)), w, h, ch, spp, gamma, None)
+    lib.convertAccumToDisplayCUDA(dacc, out.ctypes.data_as(C.POINTER(C.c_uint8)), w, h, ch, spp, gamma, counts)
     return out
 
 
-def _noalloc(dacc, w, h, ch, spp, gamma=2.0):
+def _noalloc(dacc, w, h, ch, spp, gamma=2.0, counts=None):
     out = np.full(w * h * ch, 7, np.uint8)
-    st = lib.convertAccumToDisplayNoAlloc(dacc, out.ctypes.data_as(C.POINTER(C.c_uint8)), w, h, ch, spp, gamma, None)
+    st = lib.convertAccumToDisplayNoAlloc(dacc, out.ctypes.data_as(C.POINTER(C.c_uint8)), w, h, ch, spp, gamma,
+                                          counts)
     assert st == 0, lib.rb_last_error()
     return out
 
@@ -56,6 +59,27 @@ def test_no_alloc_display_matches_existing(cuda):
         lib.freeDeviceAccumBuffer(dacc)
     lib.setBackgroundIntensity(1.0)
     ds.free()
+
+
+def test_no_alloc_counts_strip_and_free_memory(cuda):
+    torch = cuda
+    g = torch.Generator(device="cuda").manual_seed(3)
+    # a 1 x 600,000 strip: more rows than a (32 x 8)-block 2-D grid can cover
+    w, h, ch, spp = 1, 600_000, 3, 16
+    acc = torch.rand((w * h, 4), generator=g, device="cuda") * 24.0
+    # per-pixel counts: converged pixels hold negative counts, a few zeros
+    counts = torch.randint(-64, 65, (w * h,), generator=g, device="cuda", dtype=torch.int32)
+    a = _existing(C.c_void_p(acc.data_ptr()), w, h, ch, spp, counts=C.c_void_p(counts.data_ptr()))
+    b = _noalloc(C.c_void_p(acc.data_ptr()), w, h, ch, spp, counts=C.c_void_p(counts.data_ptr()))
+    np.testing.assert_array_equal(a, b)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in range(3):  # repeated calls allocate nothing
+        b2 = _noalloc(C.c_void_p(acc.data_ptr()), w, h, ch, spp, counts=C.c_void_p(counts.data_ptr()))
+        np.testing.assert_array_equal(a, b2)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
 
 
 def test_no_alloc_rejects_oversize(cuda):
