@@ -326,7 +326,18 @@ int rb_render_views_wavefront(const rb_cuda_scene *scene, int n_views, int width
                               const double *frames, int samples, int sample_base, int max_depth,
                               double *accum, int queue_capacity, uint64_t *counters, void *stream);
 
+/* Number of this library's kernel launches so far (all entry points). */
 unsigned long long rb_launch_count(void);
+
+/* Per-kernel timing for measurement (no counterpart in the reference). While
+ * enabled, each launch of the per-frame render kernel (k_render) is bracketed
+ * by two CUDA events recorded on the stream it is launched on.
+ * rb_kernel_timer_read waits for the recorded events, returns the summed
+ * elapsed milliseconds and the number of launches since the last read, and
+ * releases the events. Off by default; not for use while a stream that
+ * launches k_render is being captured into a graph. */
+void rb_kernel_timer_enable(int on);
+int rb_kernel_timer_read(double *ms, int64_t *launches);
 
 /* ======================================================================== */
 /* 4. Batched multi-job engine and serving loop (additions; the reference    */

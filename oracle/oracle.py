@@ -40,7 +40,7 @@ class Globals:
 def lib():
     global _lib
     if _lib is None:
-        from rayon_b200._native import MaterialDesc
+        from .refbind import RefMaterial as MaterialDesc
         if not OUT.exists():
             build_oracle()
         L = C.CDLL(str(OUT))
@@ -61,18 +61,40 @@ class OracleScene:
 
     def __init__(self, sc, use_bvh: bool = True, sdf: tuple | None = None) -> None:
         """sdf = (blend radius k, max steps, epsilon) for scenes with SDF primitives."""
-        from rayon_b200._native import MaterialDesc
-        L = lib()
-        self.geoms = np.ascontiguousarray(sc.export_geometry())
-        mats = sc.export_materials()
-        self._mats = (MaterialDesc * max(1, len(mats)))(*mats)
         b = sc.export_bvh()
+        self._init(sc.export_geometry(), sc.export_materials(), b if use_bvh else None, sdf)
+
+    @classmethod
+    def from_arrays(cls, spec, sdf: tuple | None = None) -> "OracleScene":
+        """A scene straight from workload arrays (materials, kinds, params,
+        mats in insertion order), traversed by linear scan: no BVH and no
+        call into this project's library."""
+        o = cls.__new__(cls)
+        kinds = np.asarray(spec.kinds)
+        g = np.zeros((kinds.shape[0], 32), np.float64)
+        # geometry kinds of the workload arrays -> Scene::GeometryType numbering
+        g[:, 0] = np.choose(kinds, [0, 1, 4, 6])
+        g[:, 1] = spec.mats
+        g[:, 2] = 1.0
+        g[:, 4:22] = spec.params
+        g[:, 31] = np.arange(kinds.shape[0])
+        o._init(g, list(spec.materials), None, sdf)
+        return o
+
+    def _init(self, geoms, mats, b, sdf) -> None:
+        from .refbind import RefMaterial, as_ref_material
+        L = lib()
+        self.geoms = np.ascontiguousarray(geoms, np.float64)
+        self._mats = (RefMaterial * max(1, len(mats)))(*[as_ref_material(m) for m in mats])
         self._b = b
-        n = b.a.shape[0] if use_bvh else 0
-        self.h = L.orc_scene_create(self.geoms.ctypes.data_as(dp), self.geoms.shape[0], self._mats, len(mats),
-                                    b.bounds.ctypes.data_as(dp), b.a.ctypes.data_as(i32p), b.b.ctypes.data_as(i32p),
-                                    b.is_leaf.ctypes.data_as(u8p), b.split_axis.ctypes.data_as(u8p), n,
-                                    b.root if use_bvh else -1)
+        if b is not None:
+            self.h = L.orc_scene_create(self.geoms.ctypes.data_as(dp), self.geoms.shape[0], self._mats, len(mats),
+                                        b.bounds.ctypes.data_as(dp), b.a.ctypes.data_as(i32p),
+                                        b.b.ctypes.data_as(i32p), b.is_leaf.ctypes.data_as(u8p),
+                                        b.split_axis.ctypes.data_as(u8p), b.a.shape[0], b.root)
+        else:
+            self.h = L.orc_scene_create(self.geoms.ctypes.data_as(dp), self.geoms.shape[0], self._mats, len(mats),
+                                        None, None, None, None, None, 0, -1)
         if sdf is not None:
             L.orc_scene_set_sdf(self.h, float(sdf[0]), int(sdf[1]), float(sdf[2]))
 
@@ -87,12 +109,16 @@ class OracleScene:
 
     def render(self, frame, w: int, h: int, spp: int, depth: int, globals_: Globals, seed: int, salt: int = 0,
                sample_base: int = 0, pixels=None, threads: int = 0):
-        """Per-pixel radiance sums (npix, 3) FP64 and counters [nodes, prims, segments, paths, shadow]."""
+        """Per-pixel radiance sums (npix, 3) FP64 and 14 work counters: nodes visited,
+        primitives tested, segments, paths, shadow rays; primitive tests by kind
+        (sphere, rectangle, triangle, SDF); shading events by class (Lambert,
+        mirror / rough mirror, glass, emitter / constant / normals, GGX
+        conductor / thin film / clear coat)."""
         fr = np.ascontiguousarray(frame, np.float64)
         px = None if pixels is None else np.ascontiguousarray(pixels, np.int32)
         n = w * h if px is None else px.shape[0]
         out = np.zeros((n, 3), np.float64)
-        cnt = np.zeros(5, np.int64)
+        cnt = np.zeros(14, np.int64)
         g = globals_.c()
         lib().orc_render(self.h, w, h, fr.ctypes.data_as(dp), None if px is None else px.ctypes.data_as(i32p), n,
                          spp, sample_base, depth, C.byref(g), seed, salt, out.ctypes.data_as(dp), threads,

@@ -106,9 +106,17 @@ struct Scene {
   double sdf_eps = 1e-4;
 };
 
+// Work counters. kind[] counts primitive tests by geometry kind (sphere and
+// displaced sphere, rectangle, triangle, SDF primitive); shade[] counts
+// shading events by resolved material class (Lambert, mirror and rough
+// mirror, glass, light and constant and normals, GGX conductor / thin film /
+// clear coat).
 struct Counters {
   int64_t nodes = 0, prims = 0, segments = 0, paths = 0, shadow = 0;
+  int64_t kind[4] = {0, 0, 0, 0};
+  int64_t shade[5] = {0, 0, 0, 0, 0};
 };
+enum { ORC_NCOUNTERS = 14 };
 
 Mat resolve(const rb_material_desc &d) {
   Mat m;
@@ -272,6 +280,15 @@ bool t_sdf_single(const Scene &S, const SdfP &q, const Ray &r, double tmin, doub
   return false;
 }
 
+int kind_slot(int type) {
+  switch (type) {
+    case RB_GEOM_SPHERE: case RB_GEOM_DISPLACED_SPHERE: return 0;
+    case RB_GEOM_RECTANGLE: return 1;
+    case RB_GEOM_TRIANGLE: return 2;
+    default: return 3;
+  }
+}
+
 bool prim_t(const Scene &S, int i, const Ray &r, double tmin, double tmax, double &t) {
   const Geom &g = S.g[i];
   switch (g.type) {
@@ -416,6 +433,7 @@ int trace_bvh(const Scene &S, const Ray &r, double tmin, double tmax, double &to
     for (int i = 0; i < (int)S.g.size(); ++i) {
       double t;
       ++c.prims;
+      ++c.kind[kind_slot(S.g[i].type)];
       if (prim_t(S, i, r, tmin, closest, t)) {
         closest = t;
         hit = i;
@@ -436,6 +454,7 @@ int trace_bvh(const Scene &S, const Ray &r, double tmin, double tmax, double &to
       for (int i = 0; i < n.b; ++i) {
         double t;
         ++c.prims;
+        ++c.kind[kind_slot(S.g[n.a + i].type)];
         if (prim_t(S, n.a + i, r, tmin, closest, t)) {
           closest = t;
           hit = n.a + i;
@@ -796,6 +815,8 @@ D3 radiance(const Scene &S, const Globals &G, Ray ray, uint32_t key, int depth, 
     }
     if (s.mat < 0 || s.mat >= (int)S.m.size()) return L;
     const Mat &m = S.m[s.mat];
+    ++c.shade[m.kind == L_LAMB ? 0 : (m.kind == L_MIRROR || m.kind == L_ROUGH) ? 1 : m.kind == L_GLASS ? 2
+              : (m.kind == L_LIGHT || m.kind == L_CONST || m.kind == L_NORMALS) ? 3 : 4];
     const Scat o = scatter(G, m, s, ray, key, bounce);
     if (o.emit.len2() > 0) {
       double w = 1;
@@ -978,7 +999,9 @@ void orc_primary(void *sp, int w, int h, const double *fr, int32_t *ids, double 
 
 // Renders samples [sample_base, sample_base + spp) for the listed pixels
 // (pixel indices y * w + x; NULL = all w*h) and writes per-pixel radiance SUMS
-// (FP64) to out (npix x 3). counters: nodes, prims, segments, paths, shadow rays.
+// (FP64) to out (npix x 3). counters (ORC_NCOUNTERS): nodes, prims, segments,
+// paths, shadow rays, primitive tests by kind (sphere, rectangle, triangle,
+// SDF), shading events by class (Lambert, mirror, glass, emitter, GGX/film/coat).
 void orc_render(void *sp, int w, int h, const double *fr, const int32_t *pixels, int npix, int spp, int sample_base,
                 int depth, const orc_globals *g, uint32_t seed, uint32_t salt, double *out, int threads,
                 int64_t *counters) {
@@ -1018,6 +1041,8 @@ void orc_render(void *sp, int w, int h, const double *fr, const int32_t *pixels,
       counters[2] += c.segments;
       counters[3] += c.paths;
       counters[4] += c.shadow;
+      for (int k = 0; k < 4; ++k) counters[5 + k] += c.kind[k];
+      for (int k = 0; k < 5; ++k) counters[9 + k] += c.shade[k];
     }
 }
 

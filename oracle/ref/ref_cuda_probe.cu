@@ -245,6 +245,10 @@ extern "C" void *refc_scene_create(const void *materials, int nmat, int mat_size
   return s;
 }
 
+// The reference's device scene pointer (CudaScene::Scene*), for calls into its
+// own extern "C" renderer interface.
+extern "C" void *refc_scene_device(void *sp) { return sp ? static_cast<RefGpuScene *>(sp)->dev : nullptr; }
+
 extern "C" void refc_scene_destroy(void *sp) {
   auto *s = static_cast<RefGpuScene *>(sp);
   if (!s) return;

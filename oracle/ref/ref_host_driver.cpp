@@ -7,7 +7,15 @@
 //      project's BVH builder can be pinned against it bit for bit;
 //   2. running the reference's multi-threaded CPU renderer RendererCPUParallel
 //      (src/rayon/cpu_renderers/renderer_cpu_parallel.hpp:25-74) on the same
-//      scene and camera as the timed CPU baseline.
+//      scene and camera as the timed CPU baseline;
+//   3. the reference's camera frame (CameraBase::initialize / buildFrame,
+//      src/rayon/camera/camera_base.hpp:47-99), so the project's camera frame
+//      and the reference-arm renders use the reference's own numbers;
+//   4. primary hits through the reference's CPU scene (CPUSceneBuilder,
+//      src/rayon/scenes/scene_builder.hpp:46-80, and each shape's hit; SDF
+//      primitives march in SDFShape::hit, cpu_shapes/sdf_shape.hpp:307-330,
+//      with SDF::rayMarch, cpu_shapes/sdf.hpp:518-566), to pin the oracle's
+//      SDF primitives.
 // Nothing here is part of the product; only tests and bench.py's CPU-baseline
 // leg load the resulting library.
 #include <fcntl.h>
@@ -17,10 +25,14 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <thread>
+#include <vector>
 
 #include "rayon_b200_scene.h"
+#include "camera/camera_base.hpp"
 #include "render/renderer_interface.hpp"
+#include "scene_builder.hpp"
 #include "renderer_cpu_parallel.hpp"
 #include "obj_loader.hpp"
 #include "scene_description.hpp"
@@ -164,6 +176,63 @@ double refh_render_cpu_parallel(void *sp, const double *look_from, const double 
   if (threads_used) *threads_used = (int)std::max(1u, std::thread::hardware_concurrency());
   if (rays_out) *rays_out = counter.load();
   return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// The reference's camera frame for (look_from, look_at, vup, vfov, w, h):
+// out = camera_center, pixel00_loc, pixel_delta_u, pixel_delta_v, u, v, w
+// (21 doubles), as CameraBase::buildFrame returns them after updateFrame.
+void refh_camera_frame(const double *look_from, const double *look_at, const double *vup, double vfov, int w, int h,
+                       double *out) {
+  CameraBase cam(Vec3(0, 0, 0), w, h, 3, 1, nullptr);
+  cam.look_from = v3(look_from);
+  cam.look_at = v3(look_at);
+  cam.vup = v3(vup);
+  cam.vfov = vfov;
+  cam.updateFrame();
+  const CameraFrame f = cam.buildFrame();
+  const Vec3 *v[7] = {&f.camera_center, &f.pixel00_loc, &f.pixel_delta_u, &f.pixel_delta_v, &f.u, &f.v, &f.w};
+  for (int k = 0; k < 7; ++k)
+    for (int c = 0; c < 3; ++c) out[3 * k + c] = (*v[k])[c];
+}
+
+// Pixel-centre primary rays (camera frame fr as above) through the
+// reference's CPU scene: closest hit over its objects in order, exactly as
+// Hittable_list::hit (data_structures/hittable_list.hpp:32-50) with
+// Interval(0.001, +inf), recording which object was hit. The ray direction is
+// normalised: SDF::rayMarch advances the ray parameter by the field value,
+// which is a distance along the ray only for a unit direction. Outputs per
+// pixel: object index or -1, t (a distance, since the direction is a unit
+// vector), the recorded normal. Returns the number of objects in the scene.
+int64_t refh_cpu_primary(void *sp, int w, int h, const double *fr, int32_t *ids, double *t_out, double *n_out) {
+  auto *s = static_cast<SceneDescription *>(sp);
+  const Hittable_list world = Scene::CPUSceneBuilder::buildCPUScene(*s);
+  const Vec3 center(fr[0], fr[1], fr[2]), p00(fr[3], fr[4], fr[5]), du(fr[6], fr[7], fr[8]), dv(fr[9], fr[10], fr[11]);
+  const int nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  auto work = [&](int tid) {
+    for (int y = tid; y < h; y += nthreads)
+      for (int x = 0; x < w; ++x) {
+        const Vec3 pc = p00 + (double)x * du + (double)y * dv;
+        const Ray r(center, unit_vector(pc - center));
+        Hit_record tmp, rec;
+        double closest = std::numeric_limits<double>::infinity();
+        int hit = -1;
+        for (size_t i = 0; i < world.objects.size(); ++i) {
+          if (world.objects[i]->hit(r, Interval(0.001, closest), tmp)) {
+            hit = (int)i;
+            closest = tmp.t;
+            rec = tmp;
+          }
+        }
+        const size_t pix = (size_t)y * w + x;
+        ids[pix] = hit;
+        t_out[pix] = hit >= 0 ? rec.t : -1.0;
+        for (int c = 0; c < 3; ++c) n_out[3 * pix + c] = hit >= 0 ? rec.normal[c] : 0.0;
+      }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 0; i < nthreads; ++i) pool.emplace_back(work, i);
+  for (auto &th : pool) th.join();
+  return (int64_t)world.objects.size();
 }
 
 }  // extern "C"

@@ -81,6 +81,8 @@ def _sig(name, res, *args):
 _sig("rb_last_error", C.c_char_p)
 _sig("rb_version", C.c_char_p)
 _sig("rb_launch_count", C.c_ulonglong)
+_sig("rb_kernel_timer_enable", None, C.c_int)
+_sig("rb_kernel_timer_read", C.c_int, c_double_p, c_int64_p)
 
 # --- drop-in group (renderer_cuda_device.cuh:8-67) ---------------------------
 _sig("initCudaStreams", None)

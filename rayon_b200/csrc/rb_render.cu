@@ -782,6 +782,20 @@ static cudaMemPool_t scratch_pool() {
   return pools[dev];
 }
 
+// Opt-in per-kernel timing (rb_kernel_timer_enable): event pairs recorded on
+// the launching stream around each k_render launch, read and released by
+// rb_kernel_timer_read.
+static std::atomic<bool> g_ktimer_on{false};
+static std::mutex g_ktimer_mu;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_ktimer_events;
+
+static cudaEvent_t ktimer_mark(cudaStream_t st) {
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  cudaEventRecord(e, st);
+  return e;
+}
+
 int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, int *counts,
                   unsigned long long *counters, cudaStream_t st) {
   const rb_render_opts o = current_opts();
@@ -824,6 +838,7 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   grd.z = slices;
 #define RB_LAUNCH(NEE_, MS_) \
   launch_ms<NEE_, MS_>(minb, grd, blk, sm, st, ds->view, G, P, acc, comp, part, counts, counters)
+  cudaEvent_t t0 = g_ktimer_on.load(std::memory_order_relaxed) ? ktimer_mark(st) : nullptr;
   if (G.nee) {
     if (ms == RB_MS_DIFFUSE) RB_LAUNCH(true, RB_MS_DIFFUSE);
     else if (ms == RB_MS_CLASSIC) RB_LAUNCH(true, RB_MS_CLASSIC);
@@ -836,6 +851,12 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
     else RB_LAUNCH(false, RB_MS_SDF);
   }
 #undef RB_LAUNCH
+  if (t0) {
+    cudaEvent_t t1 = ktimer_mark(st);
+    std::lock_guard<std::mutex> lk(g_ktimer_mu);
+    if (t1) g_ktimer_events.emplace_back(t0, t1);
+    else cudaEventDestroy(t0);
+  }
   g_launches++;
   bool ok = cuda_ok(cudaGetLastError(), "k_render launch");
   if (part) {
@@ -1425,5 +1446,30 @@ int rb_render_accumulate(const rb_cuda_scene *scene, int w, int h, const double 
 }
 
 unsigned long long rb_launch_count(void) { return g_launches.load(); }
+
+void rb_kernel_timer_enable(int on) { g_ktimer_on.store(on != 0); }
+
+int rb_kernel_timer_read(double *ms, int64_t *launches) {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  {
+    std::lock_guard<std::mutex> lk(g_ktimer_mu);
+    ev.swap(g_ktimer_events);
+  }
+  double total = 0.0;
+  int rc = RB_OK;
+  for (auto &p : ev) {
+    float m = 0.f;
+    if (cuda_ok(cudaEventSynchronize(p.second), "rb_kernel_timer_read") &&
+        cuda_ok(cudaEventElapsedTime(&m, p.first, p.second), "rb_kernel_timer_read"))
+      total += m;
+    else
+      rc = RB_ERR_CUDA;
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  if (ms) *ms = total;
+  if (launches) *launches = (int64_t)ev.size();
+  return rc;
+}
 
 }  // extern "C"

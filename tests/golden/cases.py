@@ -47,6 +47,29 @@ def mixed_materials() -> scenes.SceneSpec:
                             scenes.Camera((0, 6, 12), (0, 1, 0), (0, 1, 0), 45.0), 96, 72, 16, 8, background=0.3)
 
 
+def icospheres8() -> scenes.SceneSpec:
+    """A reduced icosphere configuration: 8 level-5 icospheres (163,840 GGX
+    triangles) from the icosphere generator's seed, 320x180, depth 8."""
+    return scenes.icospheres(seed=7, count=8, level=5, width=320, height=180, spp=64, depth=8)
+
+
+def sdf_pin(seed: int = 21) -> scenes.SceneSpec:
+    """SDF primitives of the four kinds the reference's CPU path and this
+    project both implement (sphere, box, torus, capsule), rotated, hard union."""
+    rng = np.random.default_rng(seed)
+    B = scenes._Builder()
+    for i in range(24):
+        t = i % 4
+        pos = rng.uniform(-6, 6, 3)
+        s = rng.uniform(0.6, 2.0)
+        rot = rng.uniform(0, 2 * np.pi, 3)
+        prm = {0: (s, 0, 0), 1: (s, 0.8 * s, 0.6 * s), 2: (s, 0.3 * s, 0), 3: (0.4 * s, s, 0)}[t]
+        B.sdf(t, pos, prm, rot, B.mat(S.lambertian(rng.uniform(0.2, 0.9, 3))))
+    k, p, m = B.arrays()
+    return scenes.SceneSpec("sdf_pin", B.materials, k, p, m, scenes.Camera((3, 7, 18), (0, 0, 0), (0, 1, 0), 45.0),
+                            160, 120, 4, 4, background=1.0, sdf_blend=0.0, sdf_steps=128, sdf_eps=1e-4)
+
+
 BVH_CASES = {
     "one_weekend": lambda: scenes.one_weekend(),
     "cornell": lambda: scenes.cornell(),
@@ -62,4 +85,22 @@ HIT_CASES = {
     "grid_soup": (lambda: grid_soup(), 96, 96),
     "small_icospheres": (small_icospheres, 320, 180),
     "mixed_materials": (mixed_materials, 192, 144),
+}
+
+# (case, width, height, spp, depth) of the reference CUDA renders kept for
+# converged-image RMSE checks
+REFIMG_CASES = {
+    "cornell": (lambda: scenes.cornell(), 64, 64, 4096, 16),
+    "mixed_materials": (mixed_materials, 48, 36, 4096, 8),
+    "one_weekend": (lambda: scenes.one_weekend(), 400, 225, 4096, 10),
+    "icospheres8": (icospheres8, 320, 180, 2048, 8),
+}
+
+# Per-configuration FP64 oracle ground truth on a seeded pixel subset of the
+# full frame: (case, pixels, spp). The benchmark workloads at their own sizes.
+ORACLE_PX_CASES = {
+    "one_weekend": (lambda: scenes.one_weekend(), 1024, 32768),
+    "cornell": (lambda: scenes.cornell(), 1024, 32768),
+    "icospheres": (lambda: scenes.icospheres(), 1024, 16384),
+    "sdf_field": (lambda: scenes.sdf_field(), 1024, 16384),
 }

@@ -67,3 +67,20 @@ def test_camera_frame_matches_reference_formula():
     np.testing.assert_allclose(fr[2], du, rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(fr[3], dv, rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(fr[4:7], np.stack([u, v, ww]), atol=1e-15)
+
+
+def test_camera_frame_bit_exact_against_camera_base():
+    """rb_camera_frame equals the reference's own CameraBase::buildFrame
+    (camera_base.hpp:47-99, compiled from its sources into oracle/_ref) bit for
+    bit on every workload camera, orbit views and odd aspect ratios."""
+    from oracle import refbind
+    if not refbind.host_available():
+        pytest.skip("reference drivers (oracle/_ref) not built")
+    from rayon_b200 import scenes
+    cams = [(scenes.one_weekend().camera, 400, 225), (scenes.cornell().camera, 512, 512),
+            (scenes.icospheres(count=1, level=0).camera, 1920, 1080)]
+    cams += [(v, 1280, 720) for v in scenes.sdf_field(count=2).views]
+    cams += [(scenes.orbit(scenes.cornell().camera, a), 256, 256) for a in np.linspace(0.0, 6.0, 7)]
+    cams += [(scenes.Camera((1.5, -2.0, 7.25), (0.1, 0.2, -0.3), (0.2, 1.0, 0.1), 73.0), 33, 517)]
+    for c, w, h in cams:
+        np.testing.assert_array_equal(c.frame(w, h), refbind.camera_frame(c, w, h))

@@ -91,3 +91,32 @@ def test_sdf_field_wavefront_paired_with_per_pixel_kernel(cuda, nee):
     assert bad.mean() < MAX_DIVERGED, bad.mean()
     np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=2e-2, atol=1e-3)
     ds.free()
+
+
+def test_sdf_primitives_primary_hits_vs_reference_cpu(cuda):
+    """Hard-union SDF primitives on the GPU against the reference's own CPU
+    SDF hits (SDFShape::hit, fixture tests/golden/sdf_hits_ref.npz): the same
+    object on all but grazing pixels, distances within FP32 marching error."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    from cases import sdf_pin
+    spec = sdf_pin()
+    g = np.load(Path(__file__).resolve().parent / "golden" / "sdf_hits_ref.npz")
+    w, h, fr = int(g["width"]), int(g["height"]), g["frame"]
+    sc = spec.to_scene()
+    sc.build_bvh()
+    order = sc.export_order()            # leaf position -> insertion index
+    ds = sc.upload()
+    ids, t = render.primary_hits(ds, fr, w, h, return_t=True)
+    ds.free()
+    ins = np.where(ids >= 0, order[np.maximum(ids, 0)], -1)
+    ref = g["ids"]
+    agree = (ins == ref).mean()
+    assert agree > 0.995, agree
+    both = (ins == ref) & (ref >= 0)
+    ys, xs = np.mgrid[0:h, 0:w]
+    d = fr[3:6][None, None] + xs[..., None] * fr[6:9] + ys[..., None] * fr[9:12] - fr[0:3]
+    dist = t * np.linalg.norm(d, axis=-1)
+    err = np.abs(dist - g["t"])[both]
+    assert np.percentile(err, 99) < 2e-3 and err.max() < 2e-2, (np.percentile(err, 99), err.max())

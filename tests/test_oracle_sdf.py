@@ -121,3 +121,62 @@ def test_windowed_field_matches_plain_sphere_tracing():
     both = plain_field & oracle_field
     dt = np.abs(o_t.reshape(-1)[both] - hit[both]) / il[both]  # distance along the ray
     assert np.mean(dt < 2e-3) >= 0.98, np.sort(dt)[-10:]
+
+
+def _pin_case():
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    from cases import sdf_pin
+    return sdf_pin()
+
+
+def _ray_lengths(fr, w, h):
+    ys, xs = np.mgrid[0:h, 0:w]
+    d = fr[3:6][None, None] + xs[..., None] * fr[6:9] + ys[..., None] * fr[9:12] - fr[0:3]
+    return np.linalg.norm(d, axis=-1)
+
+
+def _check_against_reference(ids, t, oids, ot, fr, w, h):
+    """Same object on every pixel; distances within the march epsilon (both
+    stop at the first point closer than 1e-4 to the surface, approaching it
+    from different starting points)."""
+    np.testing.assert_array_equal(oids, ids)
+    hit = ids >= 0
+    assert 0.15 < hit.mean() < 0.9
+    dist = ot * _ray_lengths(fr, w, h)   # the oracle's t is in units of the unnormalised ray
+    assert np.abs(dist - t)[hit].max() < 2e-4
+
+
+def test_oracle_sdf_primitives_match_reference_cpu_hits():
+    """The oracle's hard-union SDF primitives (sphere, box, torus, capsule,
+    rotated) against the reference's own CPU path: SDFShape::hit marching
+    each shape with SDF::rayMarch (cpu_shapes/sdf_shape.hpp:307-330,
+    sdf.hpp:114-160, 518-566) at its defaults (128 steps, epsilon 1e-4), on
+    the committed fixture of its pixel-centre hits (tests/golden/sdf_hits_ref.npz,
+    made by make_golden.py --sdf)."""
+    from pathlib import Path
+    spec = _pin_case()
+    g = np.load(Path(__file__).resolve().parent / "golden" / "sdf_hits_ref.npz")
+    w, h, fr = int(g["width"]), int(g["height"]), g["frame"]
+    np.testing.assert_array_equal(fr, spec.camera.frame(w, h))
+    sc = spec.to_scene()   # no BVH: geometry stays in insertion order, as the reference's object list
+    o = OracleScene(sc, use_bvh=False, sdf=(0.0, spec.sdf_steps, spec.sdf_eps))
+    oids, ot, _ = o.primary(fr, w, h)
+    _check_against_reference(g["ids"], g["t"], oids, ot, fr, w, h)
+
+
+def test_oracle_sdf_primitives_match_reference_live():
+    """As above, with the reference's CPU path run live (oracle/_ref)."""
+    import pytest
+
+    from oracle import refbind
+    if not refbind.host_available():
+        pytest.skip("reference drivers (oracle/_ref) not built")
+    spec = _pin_case()
+    w, h = spec.width, spec.height
+    fr = refbind.camera_frame(spec.camera, w, h)
+    ids, t, _ = refbind.RefScene(spec).cpu_primary(fr, w, h)
+    o = OracleScene.from_arrays(spec, sdf=(0.0, spec.sdf_steps, spec.sdf_eps))
+    oids, ot, _ = o.primary(fr, w, h)
+    _check_against_reference(ids, t, oids, ot, fr, w, h)

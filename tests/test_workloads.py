@@ -159,3 +159,38 @@ def test_orbit_keeps_radius_and_height():
         assert np.hypot(d1[0], d1[2]) == pytest.approx(np.hypot(d0[0], d0[2]))
         assert d1[1] == pytest.approx(d0[1])
         assert np.arctan2(d1[2], d1[0]) % (2 * np.pi) == pytest.approx((np.arctan2(d0[2], d0[0]) + a) % (2 * np.pi))
+
+
+@pytest.mark.parametrize("name,kw", [("one_weekend", {}), ("cornell", {}), ("icospheres", dict(count=5, level=2)),
+                                     ("sdf_field", {})])
+def test_reference_arm_generators_equal_the_workloads(name, kw):
+    """oracle/workloads.py (used by the process that drives only the reference)
+    builds the same scenes as rayon_b200/scenes.py, bit for bit."""
+    from oracle import workloads
+    a = getattr(scenes, name)(**kw)
+    b = getattr(workloads, name)(**kw)
+    np.testing.assert_array_equal(a.kinds, b.kinds)
+    np.testing.assert_array_equal(a.params, b.params)
+    np.testing.assert_array_equal(a.mats, b.mats)
+    assert len(a.materials) == len(b.materials)
+    for ma, mb in zip(a.materials, b.materials):
+        assert bytes(ma) == bytes(mb)
+    for f in ("width", "height", "spp", "depth", "background", "dof", "sdf_blend", "sdf_steps", "sdf_eps"):
+        assert getattr(a, f) == getattr(b, f), f
+    cams_a = [a.camera] + list(a.views)
+    cams_b = [b.camera] + list(b.views)
+    assert len(cams_a) == len(cams_b)
+    for ca, cb in zip(cams_a, cams_b):
+        for f in ("look_from", "look_at", "vup", "vfov"):
+            np.testing.assert_array_equal(np.asarray(getattr(ca, f), float), np.asarray(getattr(cb, f), float))
+
+
+def test_material_struct_layouts_agree():
+    """The oracle's mirror of rb_material_desc has the library's layout."""
+    import ctypes as C
+
+    from oracle.refbind import RefMaterial
+    from rayon_b200._native import MaterialDesc
+    assert C.sizeof(RefMaterial) == C.sizeof(MaterialDesc)
+    for (n1, _), (n2, _) in zip(RefMaterial._fields_, MaterialDesc._fields_):
+        assert n1 == n2 and getattr(RefMaterial, n1).offset == getattr(MaterialDesc, n2).offset
