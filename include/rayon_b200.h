@@ -229,6 +229,8 @@ typedef struct rb_upload_opts {
   int tune_depth;      /* path depth of the autotuner's probe (0 = 8) */
   int probe_width, probe_height;  /* frame size probe_frame was made for */
   const double *probe_frame;      /* autotune on this camera (rb_camera_frame), or NULL */
+  int traversal_budget;           /* testing: traversal step budget per ray (0: 2 * (primitives + 4) + 64,
+                                     which no well-formed tree reaches) */
 } rb_upload_opts;
 
 /* RB_LAYOUT_AS_BUILT: the scene's BVH as built (the reference's leaf-4 tree
@@ -257,6 +259,13 @@ rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opt
 void rb_scene_free_device(rb_cuda_scene *scene);
 /* Device bytes held by a device scene. */
 int64_t rb_scene_device_bytes(const rb_cuda_scene *scene);
+/* Rays of this scene whose BVH traversal ran out of its step budget since the
+ * upload (or the last reset): the loop then stops and the ray keeps the
+ * closest hit found so far. A well-formed tree never reaches the budget, so a
+ * nonzero count reports a corrupt tree (or a test's budget override,
+ * rb_upload_opts.traversal_budget). Waits for the device. reset != 0 zeroes
+ * the counter after reading it. */
+int rb_scene_traversal_faults(const rb_cuda_scene *scene, uint64_t *count, int reset);
 
 /* Primary hits: pixel-centre rays (no jitter, no DOF), closest hit over the
  * device BVH; ids[w*h] = leaf-order geometry index or -1; t may be NULL.
@@ -339,6 +348,15 @@ unsigned long long rb_launch_count(void);
 void rb_kernel_timer_enable(int on);
 int rb_kernel_timer_read(double *ms, int64_t *launches);
 
+/* Host-side fault injection for tests (no counterpart in the reference): the
+ * next `count` device allocations at `site` fail as if the device were out of
+ * memory, without any call into CUDA. Sites: "server_job" (a job's buffers at
+ * admission: the job is rejected with RB_ERR_OUT_OF_MEMORY, the server keeps
+ * serving the others) and "wavefront_queue" (the wavefront engine's queues:
+ * the run returns RB_ERR_OUT_OF_MEMORY and the next run allocates afresh).
+ * count 0 clears pending failures. */
+int rb_inject_alloc_failures(const char *site, int count);
+
 /* ======================================================================== */
 /* 4. Batched multi-job engine and serving loop (additions; the reference    */
 /*    renders one job per call, renderer_cuda_progressive_host.hpp:884-922)  */
@@ -398,6 +416,10 @@ typedef struct rb_job_status {
   int spp_done;
   double t_arrival, t_admit, t_done;  /* server clock, seconds */
   int64_t device_bytes;
+  int error;             /* why a rejected job was rejected: RB_ERR_CAPACITY (can never fit the
+                            budget or slots) or RB_ERR_OUT_OF_MEMORY (its buffers could not be
+                            allocated); RB_OK otherwise */
+  int reserved_;
 } rb_job_status;
 
 typedef struct rb_server_stats {

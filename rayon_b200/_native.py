@@ -59,7 +59,7 @@ class MaterialDesc(C.Structure):
 class UploadOpts(C.Structure):
     _fields_ = [("quantized_bvh", C.c_int), ("use_bvh", C.c_int), ("layout", C.c_int), ("max_leaf", C.c_int),
                 ("tune_depth", C.c_int), ("probe_width", C.c_int), ("probe_height", C.c_int),
-                ("probe_frame", C.POINTER(C.c_double))]
+                ("probe_frame", C.POINTER(C.c_double)), ("traversal_budget", C.c_int)]
 
 
 LAYOUT_AS_BUILT, LAYOUT_AUTOTUNE, LAYOUT_LINEAR, LAYOUT_LEAF = 0, 1, 2, 3
@@ -83,6 +83,7 @@ _sig("rb_version", C.c_char_p)
 _sig("rb_launch_count", C.c_ulonglong)
 _sig("rb_kernel_timer_enable", None, C.c_int)
 _sig("rb_kernel_timer_read", C.c_int, c_double_p, c_int64_p)
+_sig("rb_inject_alloc_failures", C.c_int, C.c_char_p, C.c_int)
 
 # --- drop-in group (renderer_cuda_device.cuh:8-67) ---------------------------
 _sig("initCudaStreams", None)
@@ -141,6 +142,7 @@ _sig("rb_camera_frame", None, c_double_p, c_double_p, c_double_p, C.c_double, C.
 _sig("rb_scene_upload", vp, vp, C.POINTER(UploadOpts), vp)
 _sig("rb_scene_free_device", None, vp)
 _sig("rb_scene_device_bytes", C.c_int64, vp)
+_sig("rb_scene_traversal_faults", C.c_int, vp, c_uint64_p, C.c_int)
 _sig("rb_scene_layout_info", C.c_int, vp, c_int32_p, c_int32_p, c_float_p)
 _sig("rb_primary_hits", C.c_int, vp, C.c_int, C.c_int, c_double_p, vp, vp, vp)
 _sig("rb_get_render_opts", None, C.POINTER(RenderOpts))
@@ -184,7 +186,7 @@ class ServerOpts(C.Structure):
 
 class JobStatus(C.Structure):
     _fields_ = [("state", C.c_int), ("spp_done", C.c_int), ("t_arrival", C.c_double), ("t_admit", C.c_double),
-                ("t_done", C.c_double), ("device_bytes", C.c_int64)]
+                ("t_done", C.c_double), ("device_bytes", C.c_int64), ("error", C.c_int), ("reserved_", C.c_int)]
 
 
 class ServerStats(C.Structure):

@@ -315,6 +315,7 @@ struct Job {
   float *lum = nullptr;       // mean luminance at the last convergence check (converging jobs)
   bool converged = false;
   int64_t bytes = 0;
+  int error = 0;  // rb_status of a rejection
 };
 
 struct Server {
@@ -410,14 +411,18 @@ static bool on_wavefront_scene(const Server &S, const DeviceScene *ds) {
 
 static bool on_wavefront(const Server &S, const Job &J) { return on_wavefront_scene(S, S.scenes[J.req.scene]); }
 
-static bool admit(Server &S, Job &J) {
+// 1: admitted; 0: no room now (slots or budget); -1: the job's buffers could
+// not be allocated (the device is out of memory).
+static int admit(Server &S, Job &J) {
   const bool frames = S.o.frames_every > 0;
   const int64_t need = job_bytes(J.req, frames);
-  if (S.used_bytes + need > S.o.memory_budget_bytes || (int)S.active.size() >= S.o.max_active_jobs) return false;
+  if (S.used_bytes + need > S.o.memory_budget_bytes || (int)S.active.size() >= S.o.max_active_jobs) return 0;
   const int64_t n = (int64_t)J.req.width * J.req.height;
   const bool f64 = J.req.fp64_accum || J.req.spp > 65536 || on_wavefront(S, J);
   cudaError_t e;
-  if (f64) {
+  if (injected_alloc_failure(RB_SITE_SERVER_JOB)) {
+    e = cudaErrorMemoryAllocation;
+  } else if (f64) {
     e = cudaMallocFromPoolAsync((void **)&J.acc64, n * 32, S.pool, S.st);
     if (e == cudaSuccess) e = cudaMemsetAsync(J.acc64, 0, n * 32, S.st);
   } else {
@@ -439,7 +444,8 @@ static bool admit(Server &S, Job &J) {
     if (J.frame) cudaFreeAsync(J.frame, S.st);
     if (J.lum) cudaFreeAsync(J.lum, S.st);
     J.acc = nullptr; J.acc64 = nullptr; J.frame = nullptr; J.lum = nullptr;
-    return false;
+    set_error(std::string("server: job ") + std::to_string(J.id) + " buffers: " + cudaGetErrorString(e));
+    return -1;
   }
   J.bytes = need;
   S.used_bytes += need;
@@ -447,7 +453,7 @@ static bool admit(Server &S, Job &J) {
   J.state = 1;
   J.t_admit = S.now();
   S.active.push_back(J.id);
-  return true;
+  return 1;
 }
 
 static void free_job(Server &S, Job &J) {
@@ -464,9 +470,18 @@ static int server_step(Server &S) {
   // admission: FIFO while slots and memory allow
   while (!S.queue.empty()) {
     Job &J = S.jobs[S.queue.front()];
-    if (!admit(S, J)) {
+    const int a = admit(S, J);
+    if (a < 0) {  // out of device memory: reject this job, keep serving the others
+      J.state = -1;
+      J.error = RB_ERR_OUT_OF_MEMORY;
+      S.stats.jobs_rejected++;
+      S.queue.pop_front();
+      continue;
+    }
+    if (a == 0) {
       if (S.active.empty()) {  // can never fit: reject instead of blocking the queue
         J.state = -1;
+        J.error = RB_ERR_CAPACITY;
         S.stats.jobs_rejected++;
         S.queue.pop_front();
         continue;
@@ -934,6 +949,8 @@ int rb_server_job_status(rb_server *r, int64_t id, rb_job_status *out) {
   out->t_admit = J.t_admit;
   out->t_done = J.t_done;
   out->device_bytes = J.bytes;
+  out->error = J.error;
+  out->reserved_ = 0;
   return RB_OK;
 }
 

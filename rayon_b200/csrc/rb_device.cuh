@@ -159,8 +159,19 @@ struct SceneView {
   float light_area;    // total emitter area
   float sdf_k;         // smooth-union radius
   float sdf_eps;
-  float pad_;
+  int trav_budget;     // traversal step budget override (0: 2 * (prims + 4) + 64)
+  // Rays whose traversal ran out of its step budget (a corrupt tree; never a
+  // well-formed one): counted here, read by rb_scene_traversal_faults.
+  unsigned long long *faults;
 };
+
+__device__ __forceinline__ int traversal_budget(const SceneView &S) {
+  return S.trav_budget > 0 ? S.trav_budget : 2 * (S.num_prims + 4) + 64;
+}
+
+__device__ __forceinline__ void note_budget_exhausted(const SceneView &S, int budget) {
+  if (budget <= 0 && S.faults) atomicAdd(S.faults, 1ull);
+}
 
 // Reference __constant__ settings (renderer_cuda_device.cu:18-26), passed by value.
 struct Globals {
@@ -454,7 +465,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
     return h;
   int cur = S.root_ref;
   st.sp = 0;
-  int budget = 2 * (S.num_prims + 4) + 64;  // bounds a corrupt tree (see trace_ww)
+  int budget = traversal_budget(S);  // bounds a corrupt tree (see trace_ww)
   while (--budget > 0) {
     if (ref_is_leaf(cur)) {
       const int first = leaf_first(cur), cnt = leaf_count(cur);
@@ -523,6 +534,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
     }
     if (!found) break;
   }
+  note_budget_exhausted(S, budget);
   return h;
 }
 
@@ -607,7 +619,7 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
   int leaf = RB_TRAV_DONE;  // postponed leaf
   // every interior node and every leaf is visited at most once, so this
   // budget is never reached by a well-formed tree; it bounds a corrupt one
-  int budget = 2 * (S.num_prims + 4) + 64;
+  int budget = traversal_budget(S);
   while ((node != RB_TRAV_DONE || leaf != RB_TRAV_DONE) && --budget > 0) {
     // interior phase
     while (node != RB_TRAV_DONE && !ref_is_leaf(node) && --budget > 0) {
@@ -644,6 +656,7 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
       }
     }
   }
+  note_budget_exhausted(S, budget);
   return h;
 }
 

@@ -107,6 +107,12 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
 
 bool cuda_ok(cudaError_t e, const char *what);
 void set_error(const std::string &msg);
+
+// Host-side fault injection (rb_inject_alloc_failures): the next n device
+// allocations at a site fail as if the device were out of memory. Consumes
+// one pending failure and returns true when the allocation must fail.
+enum AllocSite { RB_SITE_SERVER_JOB = 0, RB_SITE_WAVEFRONT = 1, RB_SITE_COUNT = 2 };
+bool injected_alloc_failure(int site);
 DeviceScene *lookup_scene(const void *handle);
 void build_quantized(HostLayout &L);
 FrameF frame_from(const double *fr, int w, int h);

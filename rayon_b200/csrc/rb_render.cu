@@ -434,10 +434,16 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
   v.sdf_k = hs.sdf.blend_k;
   for (int k = 0; k < 6; ++k) v.root_box[k] = L.root_box[k];
   v.light_area = L.light_area;
+  v.trav_budget = opts.traversal_budget > 0 ? opts.traversal_budget : 0;
   // The handle is a small device allocation so that it is a genuine device
   // pointer, as CudaScene::Scene* is in the reference (scene_builder_cuda.cu:294-296).
+  // It holds a copy of the view and, in its last 8 bytes, the scene's
+  // traversal-fault counter.
+  static_assert(sizeof(SceneView) <= 248, "scene view must leave room for the fault counter");
   ok = ok && cuda_ok(cudaMalloc(&ds->handle, 256), "cudaMalloc(scene handle)") &&
-       cuda_ok(cudaMemcpyAsync(ds->handle, &v, sizeof v, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(handle)") &&
+       cuda_ok(cudaMemsetAsync(ds->handle, 0, 256, st), "cudaMemsetAsync(handle)");
+  if (ok) v.faults = reinterpret_cast<unsigned long long *>(static_cast<char *>(ds->handle) + 248);
+  ok = ok && cuda_ok(cudaMemcpyAsync(ds->handle, &v, sizeof v, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync(handle)") &&
        cuda_ok(cudaStreamSynchronize(st), "cudaStreamSynchronize(upload)");
   ds->bytes = bytes + 256;
   ds->ms = L.ms;
@@ -782,6 +788,16 @@ static cudaMemPool_t scratch_pool() {
   return pools[dev];
 }
 
+static std::atomic<int> g_alloc_fail[RB_SITE_COUNT];
+
+bool injected_alloc_failure(int site) {
+  if (site < 0 || site >= RB_SITE_COUNT) return false;
+  int n = g_alloc_fail[site].load();
+  while (n > 0)
+    if (g_alloc_fail[site].compare_exchange_weak(n, n - 1)) return true;
+  return false;
+}
+
 // Opt-in per-kernel timing (rb_kernel_timer_enable): event pairs recorded on
 // the launching stream around each k_render launch, read and released by
 // rb_kernel_timer_read.
@@ -998,6 +1014,7 @@ struct TuneChoice {
   bool linear;
   int leaf;    // BVH leaf size
   int groups;  // > 0: grouped linear layout with groups of at most this many primitives
+  float probe_ms = 0.0f;  // the probe time that decided it
 };
 static std::unordered_map<TuneKey, TuneChoice, TuneKeyHash> g_tune_cache;
 
@@ -1072,6 +1089,7 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
     ds->layout_kind = c.linear ? RB_LAYOUT_LINEAR : c.groups > 0 ? RB_LAYOUT_GROUPS : RB_LAYOUT_LEAF;
     ds->layout_leaf = c.groups > 0 ? c.groups : c.leaf;
     if (cands.size() == 1) {  // cached (or only) choice: no probing
+      ds->probe_ms = c.probe_ms;
       best = ds;
       break;
     }
@@ -1093,7 +1111,7 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
     std::lock_guard<std::mutex> lk(g_mu);
     const bool groups = best->layout_kind == RB_LAYOUT_GROUPS;
     g_tune_cache[key] = {best->layout_kind == RB_LAYOUT_LINEAR, groups ? 0 : best->layout_leaf,
-                         groups ? best->layout_leaf : 0};
+                         groups ? best->layout_leaf : 0, best->probe_ms};
   }
   return best;
 }
@@ -1403,6 +1421,21 @@ void rb_scene_free_device(rb_cuda_scene *scene) {
   free_device_scene(ds);
 }
 
+int rb_scene_traversal_faults(const rb_cuda_scene *scene, uint64_t *count, int reset) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) {
+    set_error("rb_scene_traversal_faults: unknown scene handle");
+    return RB_ERR_NOT_FOUND;
+  }
+  unsigned long long n = 0;
+  if (!cuda_ok(cudaDeviceSynchronize(), "rb_scene_traversal_faults") ||
+      !cuda_ok(cudaMemcpy(&n, ds->view.faults, sizeof n, cudaMemcpyDeviceToHost), "rb_scene_traversal_faults"))
+    return RB_ERR_CUDA;
+  if (reset && !cuda_ok(cudaMemset(ds->view.faults, 0, sizeof n), "rb_scene_traversal_faults")) return RB_ERR_CUDA;
+  if (count) *count = n;
+  return RB_OK;
+}
+
 int64_t rb_scene_device_bytes(const rb_cuda_scene *scene) {
   DeviceScene *ds = lookup_scene(scene);
   return ds ? (int64_t)ds->bytes : 0;
@@ -1448,6 +1481,18 @@ int rb_render_accumulate(const rb_cuda_scene *scene, int w, int h, const double 
 unsigned long long rb_launch_count(void) { return g_launches.load(); }
 
 void rb_kernel_timer_enable(int on) { g_ktimer_on.store(on != 0); }
+
+int rb_inject_alloc_failures(const char *site, int count) {
+  if (!site || count < 0) return RB_ERR_INVALID_ARG;
+  const std::string s(site);
+  const int k = s == "server_job" ? RB_SITE_SERVER_JOB : s == "wavefront_queue" ? RB_SITE_WAVEFRONT : -1;
+  if (k < 0) {
+    set_error("rb_inject_alloc_failures: unknown site (server_job, wavefront_queue)");
+    return RB_ERR_INVALID_ARG;
+  }
+  g_alloc_fail[k].store(count);
+  return RB_OK;
+}
 
 int rb_kernel_timer_read(double *ms, int64_t *launches) {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;

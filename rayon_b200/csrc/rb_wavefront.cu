@@ -629,6 +629,10 @@ static bool wf_alloc_march(WfEngine &E) {
 static bool wf_alloc(WfEngine &E, int capacity) {
   std::memset(&E.q, 0, sizeof E.q);
   E.capacity = capacity;
+  if (injected_alloc_failure(RB_SITE_WAVEFRONT)) {
+    set_error("wavefront queue: out of memory (injected)");
+    return false;
+  }
   bool ok = true;
   for (int i = 0; i < 2 && ok; ++i) {
     ok = cuda_ok(cudaMalloc(&E.q[i].o, sizeof(float4) * capacity), "wavefront queue") &&

@@ -221,7 +221,7 @@ class SceneDescription:
 
     # --- device --------------------------------------------------------------------
     def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None, layout: str = "as_built",
-               max_leaf: int = 0, tune_depth: int = 0, probe=None) -> "DeviceScene":
+               max_leaf: int = 0, tune_depth: int = 0, probe=None, traversal_budget: int = 0) -> "DeviceScene":
         """layout: "as_built" (the built BVH; bit-exact primary hits), "autotune"
         (fastest of linear / groups of 8, 16 / leaf 1, 2, 4, 8 on a probe render),
         "linear", "leaf" (rebuilt with max_leaf), "groups" (the built BVH's subtrees of
@@ -232,6 +232,7 @@ class SceneDescription:
         o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3, "groups": 4}[layout]
         o.max_leaf = int(max_leaf)
         o.tune_depth = int(tune_depth)
+        o.traversal_budget = int(traversal_budget)
         keep = None
         if probe is not None:  # (frame[21], width, height): autotune on this camera
             keep = np.ascontiguousarray(probe[0], np.float64)
@@ -259,6 +260,12 @@ class DeviceScene:
         lib.rb_scene_layout_info(self.handle, C.byref(k), C.byref(leaf), C.byref(ms))
         kind = {2: "linear", 4: "groups"}.get(k.value, "bvh")
         return {"kind": kind, "leaf": leaf.value, "probe_ms": ms.value}
+
+    def traversal_faults(self, reset: bool = False) -> int:
+        """Rays whose BVH traversal ran out of its step budget (0 for a well-formed tree)."""
+        n = C.c_uint64(0)
+        check(lib.rb_scene_traversal_faults(self.handle, C.byref(n), int(reset)), "rb_scene_traversal_faults")
+        return int(n.value)
 
     def free(self) -> None:
         if self.handle:

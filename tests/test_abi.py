@@ -84,3 +84,10 @@ def test_camera_frame_bit_exact_against_camera_base():
     cams += [(scenes.Camera((1.5, -2.0, 7.25), (0.1, 0.2, -0.3), (0.2, 1.0, 0.1), 73.0), 33, 517)]
     for c, w, h in cams:
         np.testing.assert_array_equal(c.frame(w, h), refbind.camera_frame(c, w, h))
+
+
+def test_fault_injection_sites_are_checked():
+    assert lib.rb_inject_alloc_failures(b"no_such_site", 1) == -1
+    assert lib.rb_inject_alloc_failures(b"server_job", -2) == -1
+    assert lib.rb_inject_alloc_failures(b"server_job", 0) == 0
+    assert lib.rb_inject_alloc_failures(b"wavefront_queue", 0) == 0
