@@ -432,9 +432,9 @@ WORKLOADS = {
 # engine per workload: the per-pixel / batched kernel, or the wavefront engine
 # (whose separate field-march kernel is the faster one for SDF fields)
 ENGINE = {"sdf_field": "wavefront"}
-# wavefront queue: 16 M path slots (about 10 GB with the SDF march buffers);
-# 4 M -> 8 M -> 16 M measured 513 -> 537 -> 545 Mpaths/s on the SDF field
-WF_QUEUE = 1 << 24
+# wavefront queue: 0 = the path slots the autotuner chose for the scene
+# (2 M to 16 M; 16 M slots take about 14 GB with the SDF march buffers)
+WF_QUEUE = 0
 
 
 def workload_spec(name: str, small: bool = False):
@@ -456,6 +456,8 @@ def main():
     ap.add_argument("--workload", default="cornell", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the equal-RMSE and serving sections")
+    ap.add_argument("--serving-jobs", type=int, default=400,
+                    help="jobs of the serving section's stream (2000 = the full specified stream, ~15 min)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case for ncu: same frame at 16 spp (two views at most), no e2e/baselines")
     args = ap.parse_args()
@@ -631,6 +633,7 @@ def main():
                                       "autotune of the scene (layout_autotune_s) runs at its first upload"}}
         mean_rad = float(np.asarray(img).reshape(-1, 3).mean() / spp)
 
+    split = sample_split_section(ds, fr, w, h, spp, depth, spec, engine, world) if world > 1 else None
     peaks, peaks_kind = measured_peaks()
     res = {
         "metric": f"Mpaths/s ({desc})" if args.workload != "cornell" else METRIC,
@@ -642,7 +645,7 @@ def main():
                               "for all views)" if engine == "wavefront" else
                               "k_batch (persistent, one launch for all views)" if nviews > 1 else
                               "k_render (per-pixel, flattened sample x bounce loop)"),
-                   "layout": layout,
+                   "layout": layout, "tuning": ds.tuning,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "mrays_per_s": world * segs / (t_ms * 1e-3) / 1e6,
         "segments_per_path": segs / max(npaths, 1),
@@ -650,6 +653,8 @@ def main():
         "gpu_launches": int(launches),
         "e2e": e2e,
     }
+    if split is not None:
+        res["sample_split"] = split
     clocks = clk.summary()
     res["clocks"] = clocks
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
@@ -668,7 +673,7 @@ def main():
     res["mean_radiance"] = mean_rad
     if rank == 0 and world == 1 and args.workload == "cornell" and not args.small and not args.no_extras:
         for key, fn in (("equal_rmse", lambda: equal_rmse_section(t_ms, paths)),
-                        ("serving", lambda: serving_section())):
+                        ("serving", lambda: serving_section(args.serving_jobs))):
             try:
                 res[key] = fn()
             except Exception as e:  # noqa: BLE001
@@ -677,6 +682,41 @@ def main():
         print(json.dumps(res))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def sample_split_section(ds, fr, w, h, spp, depth, spec, engine, world):
+    """One frame of the workload split by samples over the ranks
+    (multigpu.render_sample_split: rank r renders its sample range with the
+    per-frame kernel, then one FP64 all-reduce over NCCL), timed with CUDA
+    events between barriers, max over ranks: the strong-scaling form of the
+    path next to the replicas of the main line. Rank 0 checks the reduced
+    image against its own render of all the samples."""
+    import torch
+    import torch.distributed as dist
+
+    from rayon_b200 import multigpu, render
+    if engine != "kernel":
+        return {"unavailable": "the sample split drives the per-frame kernel"}
+    run = multigpu.gpu_range_renderer(ds, fr, w, h, depth, background=spec.background, dof=spec.dof)
+    multigpu.render_sample_split(run, spp)          # warm-up (same collective steps on every rank)
+    dist.barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    total = multigpu.render_sample_split(run, spp)
+    b.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([a.elapsed_time(b)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    out = {"ms_per_frame": ms, "mpaths_s": w * h * spp / (ms * 1e-3) / 1e6, "ranks": world,
+           "collective": "one FP64 all-reduce of the frame's sums (NCCL)"}
+    if dist.get_rank() == 0:
+        ref = render.render_accumulate(ds, fr, w, h, spp, depth, background=spec.background,
+                                       dof=spec.dof).reshape(-1, 3)
+        got = total.cpu().numpy()
+        out["max_rel_diff_vs_one_gpu"] = float(np.max(np.abs(got - ref) / (1.0 + np.abs(ref))))
+    return out
 
 
 def quantized_compare(sc, fr, w, h, spp, depth, step_ms):
@@ -743,18 +783,24 @@ def reference_cuda(spec):
                     "e2e excludes its scene build and upload (scene_build_upload_s)"}
 
 
-def serving_section(n_jobs: int = 40, rate: float = 50.0):
-    """The serving mix (scaled down from 2000 jobs): Poisson arrivals at `rate`
-    jobs/s over the one-weekend, Cornell, icosphere and SDF scenes, resolutions
-    from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform [16, 1024], orbit
-    angle U[0, 2pi). Plain = each job as its own per-frame launch, back to back;
-    served = the batched serving loop with real-time arrivals; backlog = the
-    same jobs all queued at once."""
+def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False):
+    """The serving mix: n_jobs Poisson arrivals at `rate` jobs/s (2000 in the
+    specified stream) over the One-Weekend, Cornell, icosphere and SDF scenes,
+    resolutions from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform
+    [16, 1024], orbit angle U[0, 2pi).
+
+    plain: each job as its own per-frame launch, back to back, into one
+    accumulation buffer allocated once, each launch timed with CUDA events
+    (device seconds) and the loop on the wall clock; served: the batched
+    serving loop with real-time arrivals (wall clock; device seconds from the
+    server's own events); backlog (optional): the same jobs all queued at
+    once. Ratios are wall/wall and device/device."""
     import torch
 
     from rayon_b200 import lib, render, scenes, serving
     t0 = time.time()
     specs = [scenes.one_weekend(), scenes.cornell(), scenes.icospheres(), scenes.sdf_field()]
+    names = ["one_weekend", "cornell", "icospheres", "sdf_field"]
     dss = []
     for sp in specs:
         sc = sp.to_scene()
@@ -765,26 +811,39 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
     mix = scenes.serving_mix(n_jobs, rate=rate, n_scenes=len(specs))
     frames = [scenes.orbit(specs[j["scene"]].camera, j["angle"]).frame(j["width"], j["height"]) for j in mix]
     paths = sum(j["width"] * j["height"] * j["spp"] for j in mix)
-    # clocks over each of the three runs (the section follows minutes of load)
+    scene_paths = [sum(j["width"] * j["height"] * j["spp"] for j in mix if j["scene"] == i) for i in range(4)]
     clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))).__enter__()
     clocks = {}
-    # plain per-job launches
+    # plain per-job launches into one pre-allocated buffer
+    maxpx = max(j["width"] * j["height"] for j in mix)
+    acc = torch.zeros((2 * maxpx, 4), device="cuda")
+    scene_dev = [0.0] * 4
+    evs = []
     torch.cuda.synchronize()
     tp = time.time()
     clk.mark(True)
     for j, fr in zip(mix, frames):
         sp = specs[j["scene"]]
+        n = j["width"] * j["height"]
         render.set_globals(background=sp.background, dof=sp.dof)
-        acc = torch.zeros((j["width"] * j["height"] * 2, 4), device="cuda")
+        acc[:2 * n].zero_()
         frc = np.ascontiguousarray(fr)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
         lib.rb_render_accumulate(dss[j["scene"]].handle, j["width"], j["height"],
                                  frc.ctypes.data_as(C.POINTER(C.c_double)), j["spp"], 0, sp.depth,
-                                 C.c_void_p(acc.data_ptr()), C.c_void_p(acc.data_ptr() + j["width"] * j["height"] * 16),
-                                 None, None)
-        torch.cuda.synchronize()
-    plain = time.time() - tp
+                                 C.c_void_p(acc.data_ptr()), C.c_void_p(acc.data_ptr() + n * 16), None,
+                                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        b.record()
+        evs.append((j["scene"], a, b))
+    torch.cuda.synchronize()
+    plain_wall = time.time() - tp
     clk.mark(False)
+    for sidx, a, b in evs:
+        scene_dev[sidx] += a.elapsed_time(b) * 1e-3
+    plain_dev = sum(scene_dev)
     render.set_globals()
+    del acc
     srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
     ids = [srv.add_scene(ds) for ds in dss]
     reqs = [serving.job(ids[j["scene"]], fr, j["width"], j["height"], j["spp"], specs[j["scene"]].depth,
@@ -792,26 +851,30 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
             for k, (j, fr) in enumerate(zip(mix, frames))]
     tb = time.time()
     srv.run_trace(reqs, realtime=True)
-    wall = time.time() - tb
+    served_wall = time.time() - tb
     clk_t = (tb, time.time())
     st = srv.stats()
     srv.close()
-    # the same jobs as one backlog (all queued at once): the loop's throughput
-    # without the arrival ramp of the real-time trace
-    srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
-    ids = [srv.add_scene(ds) for ds in dss]
-    for r, j in zip(reqs, mix):
-        r.scene = ids[j["scene"]]
-        r.arrival_time = 0.0
-    tb = time.time()
-    srv.run_trace(reqs, realtime=False)
-    wall_backlog = time.time() - tb
-    clk_b = (tb, time.time())
-    st_backlog = srv.stats()
-    srv.close()
+    out_backlog = {}
+    clk_b = None
+    if backlog:  # the same jobs all queued at once: the loop's throughput without the arrival ramp
+        srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
+        ids = [srv.add_scene(ds) for ds in dss]
+        for r, j in zip(reqs, mix):
+            r.scene = ids[j["scene"]]
+            r.arrival_time = 0.0
+        tb = time.time()
+        srv.run_trace(reqs, realtime=False)
+        wall_b = time.time() - tb
+        clk_b = (tb, time.time())
+        sb = srv.stats()
+        srv.close()
+        out_backlog = {"backlog_mpaths_s_wall": paths / wall_b / 1e6,
+                       "backlog_mpaths_s_device": sb.paths / sb.device_seconds / 1e6 if sb.device_seconds else None}
     clk.__exit__(None, None, None)
     path_csv = clk.path
-    for name, (a, b) in (("plain", (clk.t0, clk.t1)), ("served", clk_t), ("backlog", clk_b)):
+    runs = [("plain", (clk.t0, clk.t1)), ("served", clk_t)] + ([("backlog", clk_b)] if clk_b else [])
+    for name, (a, b) in runs:
         c = ClockSampler(clk.gpu)
         c.path, c.t0, c.t1 = path_csv, a, b
         clocks[name] = c.summary(keep=True)
@@ -819,18 +882,25 @@ def serving_section(n_jobs: int = 40, rate: float = 50.0):
         os.unlink(path_csv)
     for ds in dss:
         ds.free()
-    return {"jobs": n_jobs, "arrival_rate_per_s": rate, "paths": paths,
-            "offered_gpaths_per_s": paths / mix[-1]["t"] / 1e9,
-            "plain_per_job_mpaths_s": paths / plain / 1e6,
-            "served_mpaths_s_wall": paths / wall / 1e6,
-            "served_mpaths_s_device": st.paths / st.device_seconds / 1e6 if st.device_seconds else None,
-            "backlog_mpaths_s_device": (st_backlog.paths / st_backlog.device_seconds / 1e6
-                                        if st_backlog.device_seconds else None),
-            "backlog_mpaths_s_wall": paths / wall_backlog / 1e6,
-            "p50_latency_s": st.p50_latency, "p99_latency_s": st.p99_latency, "mean_latency_s": st.mean_latency,
-            "iterations": st.iterations, "peak_device_bytes": st.peak_device_bytes, "setup_s": setup,
-            "clocks": clocks,
-            "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}
+    served_dev = st.device_seconds
+    res = {"jobs": n_jobs, "arrival_rate_per_s": rate, "paths": paths, "arrival_window_s": mix[-1]["t"],
+           "offered_gpaths_per_s": paths / mix[-1]["t"] / 1e9,
+           "plain_mpaths_s_wall": paths / plain_wall / 1e6, "plain_mpaths_s_device": paths / plain_dev / 1e6,
+           "served_mpaths_s_wall": paths / served_wall / 1e6,
+           "served_mpaths_s_device": st.paths / served_dev / 1e6 if served_dev else None,
+           "served_over_plain_wall": plain_wall / served_wall,
+           "served_over_plain_device": plain_dev / served_dev if served_dev else None,
+           "p50_latency_s": st.p50_latency, "p99_latency_s": st.p99_latency, "mean_latency_s": st.mean_latency,
+           "jobs_done": st.jobs_done, "jobs_rejected": st.jobs_rejected,
+           "iterations": st.iterations, "peak_device_bytes": st.peak_device_bytes, "setup_s": setup,
+           "plain_by_scene": {nm: {"path_share": scene_paths[i] / paths,
+                                   "plain_mpaths_s_device": scene_paths[i] / scene_dev[i] / 1e6 if scene_dev[i] else None,
+                                   "plain_time_share": scene_dev[i] / plain_dev}
+                              for i, nm in enumerate(names)},
+           "clocks": clocks,
+           "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}
+    res.update(out_backlog)
+    return res
 
 
 def equal_rmse_section(full_ms_plain: float, full_paths: int):

@@ -253,6 +253,23 @@ enum { RB_LAYOUT_AS_BUILT = 0, RB_LAYOUT_AUTOTUNE = 1, RB_LAYOUT_LINEAR = 2, RB_
  * the probe time of the winner. */
 int rb_scene_layout_info(const rb_cuda_scene *scene, int *kind, int *leaf, float *probe_ms);
 
+/* Everything the autotuner (RB_LAYOUT_AUTOTUNE) chose for a scene. Decisions
+ * are cached per (GPU, scene fingerprint): a second upload of the same scene
+ * on the same GPU reuses them without probing (from_cache = 1). Zeros mean
+ * the class defaults (an upload that was not autotuned). */
+typedef struct rb_tuning {
+  int layout;           /* RB_LAYOUT_LINEAR, RB_LAYOUT_LEAF or RB_LAYOUT_GROUPS */
+  int leaf;             /* BVH leaf size or group size (0 for linear) */
+  int blocks_per_sm;    /* per-frame kernel: resident 256-thread blocks per SM (register budget) */
+  int block_x, block_y; /* per-frame kernel: block shape */
+  int short_stack;      /* traversal stack entries kept in shared memory */
+  int wavefront_queue;  /* wavefront engine path slots (smooth-SDF scenes; 0: not tuned) */
+  float probe_ms;       /* probe time of the chosen configuration */
+  int from_cache;       /* 1: the decision came from the per-(GPU, scene) cache */
+  int reserved_[3];
+} rb_tuning;
+int rb_scene_tuning(const rb_cuda_scene *scene, rb_tuning *out);
+
 /* Upload to the current device. Returns an opaque device-scene handle that is
  * also accepted wherever the drop-in group takes a CudaScene::Scene*. */
 rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opts, void *stream);

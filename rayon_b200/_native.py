@@ -144,6 +144,16 @@ _sig("rb_scene_free_device", None, vp)
 _sig("rb_scene_device_bytes", C.c_int64, vp)
 _sig("rb_scene_traversal_faults", C.c_int, vp, c_uint64_p, C.c_int)
 _sig("rb_scene_layout_info", C.c_int, vp, c_int32_p, c_int32_p, c_float_p)
+
+
+class Tuning(C.Structure):
+    """rb_tuning: what the autotuner chose for a scene."""
+    _fields_ = [("layout", C.c_int), ("leaf", C.c_int), ("blocks_per_sm", C.c_int), ("block_x", C.c_int),
+                ("block_y", C.c_int), ("short_stack", C.c_int), ("wavefront_queue", C.c_int),
+                ("probe_ms", C.c_float), ("from_cache", C.c_int), ("reserved_", C.c_int * 3)]
+
+
+_sig("rb_scene_tuning", C.c_int, vp, C.POINTER(Tuning))
 _sig("rb_primary_hits", C.c_int, vp, C.c_int, C.c_int, c_double_p, vp, vp, vp)
 _sig("rb_get_render_opts", None, C.POINTER(RenderOpts))
 _sig("rb_set_render_opts", None, C.POINTER(RenderOpts))

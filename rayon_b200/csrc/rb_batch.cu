@@ -94,9 +94,10 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
   jobs += ctl->job_offset;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
+  // shared stack entries: as many as the launch provided (the largest of its
+  // jobs' scenes' short_stack)
   Stack st;
-  st.sh = smem + tid;
-  st.stride = blockDim.x;
+  stack_init(st, smem, tid, blockDim.x, RB_SHORT_MAX);
   uint32_t ovf = 0;
   const unsigned long long total = ctl->total_tasks;
   const int njobs = ctl->njobs;
@@ -172,19 +173,26 @@ __global__ void __launch_bounds__(256, MINB) k_batch(const BatchJob *__restrict_
         }
       }
       if (alive) {
-        // the whole path at once: a lane whose path ends early waits for the
-        // warp's longest, and the warp's next camera rays start together
-        // (coherent), as in the per-frame kernel's sample loop
+        // Diffuse scenes (Lambert walls, long paths of geometrically
+        // distributed length): one segment per pass of the outer loop, so a
+        // lane whose path ends starts its next sample (or claims its next
+        // task) at once, as the per-frame kernel's flattened loop does. The
+        // other classes trace the whole path at once: a lane whose path ends
+        // early waits for the warp's longest, and the warp's next camera rays
+        // start together (coherent).
+        constexpr bool kFlat = MS == RB_MS_DIFFUSE;
         bool end = false;
-        while (!end) {
+        do {
           ++segs;
           end = path_segment<NEE, MS>(job_or_uniform<UNI>(Su, J.S), job_or_uniform<UNI>(Gu, J.G), st, ovf, ray, thr, L,
                                       bounce, prev_pdf, key, J.P.max_depth);
+        } while (!kFlat && !end);
+        if (end) {
+          kahan_add(sx, cx, L.x);
+          kahan_add(sy, cy, L.y);
+          kahan_add(sz, cz, L.z);
+          alive = false;
         }
-        kahan_add(sx, cx, L.x);
-        kahan_add(sy, cy, L.y);
-        kahan_add(sz, cz, L.z);
-        alive = false;
       }
     }
   }
@@ -228,8 +236,8 @@ template <int MS, bool NEE>
 // uni (may be null): the scene and settings every job of the launch shares;
 // the uniform variant exists for the default occupancy (4 blocks per SM).
 static void launch_batch_ms(int minb, int grid, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl,
-                            const BatchUniform *uni) {
-  const size_t sm = sizeof(int2) * RB_SHORT * 256;
+                            const BatchUniform *uni, int short_stack) {
+  const size_t sm = stack_smem_bytes(short_stack, 256);
   if (uni && minb == 4) {
     k_batch<MS, 4, NEE, true><<<grid, 256, sm, st>>>(jobs, ctl, uni->S, uni->G);
     return;
@@ -258,19 +266,20 @@ static int batch_minb(int ms, bool nee) {
 
 // One persistent launch for a class group; the next-event-estimation variant
 // only when a job of the group asks for it (it costs registers).
+// short_stack: the largest SceneView::short_stack among the launch's jobs.
 static void launch_batch(int ms, int minb, bool nee, cudaStream_t st, const BatchJob *jobs, BatchCtl *ctl, int sms,
-                         const BatchUniform *uni) {
+                         const BatchUniform *uni, int short_stack) {
   const int grid = sms * minb;  // persistent: exactly the resident blocks
   if (nee) {
-    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, true>(minb, grid, st, jobs, ctl, uni);
-    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, true>(minb, grid, st, jobs, ctl, uni);
-    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, true>(minb, grid, st, jobs, ctl, uni);
-    else launch_batch_ms<RB_MS_SDF, true>(minb, grid, st, jobs, ctl, uni);
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, true>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, true>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, true>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else launch_batch_ms<RB_MS_SDF, true>(minb, grid, st, jobs, ctl, uni, short_stack);
   } else {
-    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, false>(minb, grid, st, jobs, ctl, uni);
-    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, false>(minb, grid, st, jobs, ctl, uni);
-    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, false>(minb, grid, st, jobs, ctl, uni);
-    else launch_batch_ms<RB_MS_SDF, false>(minb, grid, st, jobs, ctl, uni);
+    if (ms == RB_MS_DIFFUSE) launch_batch_ms<RB_MS_DIFFUSE, false>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else if (ms == RB_MS_CLASSIC) launch_batch_ms<RB_MS_CLASSIC, false>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else if (ms == RB_MS_FULL) launch_batch_ms<RB_MS_FULL, false>(minb, grid, st, jobs, ctl, uni, short_stack);
+    else launch_batch_ms<RB_MS_SDF, false>(minb, grid, st, jobs, ctl, uni, short_stack);
   }
   g_launches++;
 }
@@ -329,6 +338,9 @@ struct Server {
   std::vector<int64_t> active;
   int64_t next_id = 0;
   int64_t used_bytes = 0, peak_bytes = 0;
+  // path slots of the wavefront engine: one capacity for all of the server's
+  // smooth-SDF scenes (the largest tuned one), so that runs never reallocate
+  int wf_cap = 0;
   BatchJob *h_jobs = nullptr;  // pinned
   BatchJob *d_jobs = nullptr;
   BatchCtl *h_ctl = nullptr;   // pinned
@@ -405,6 +417,8 @@ __global__ void k_job_converge(const float4 *__restrict__ acc, const double *__r
 // SDF march buffers, held for the process beside the jobs' HBM budget);
 // 4 M -> 8 M measured +4.6 % on the SDF field.
 #define RB_SERVER_WF_QUEUE (1 << 23)
+// the scene's autotuned path slots when it has them
+static int scene_wf_queue(const DeviceScene *ds) { return ds->wf_queue > 0 ? ds->wf_queue : RB_SERVER_WF_QUEUE; }
 static bool on_wavefront_scene(const Server &S, const DeviceScene *ds) {
   return S.o.wavefront_field && ds->ms >= RB_MS_SDF && ds->view.sdf_k > 0.0f && ds->view.num_sdf > 0;
 }
@@ -611,7 +625,10 @@ static int server_step(Server &S) {
       u.S = S.scenes[uni_scene[grp]]->view;
       u.G = uni_G[grp];
     }
-    launch_batch(cls, minb_of(grp), grp > 4, S.st, S.d_jobs, S.d_ctl + grp, S.sms, uniform ? &u : nullptr);
+    int stack = 0;
+    for (const auto &pl : plan)
+      if (pl.cls == grp) stack = std::max(stack, S.scenes[S.jobs[pl.id].req.scene]->view.short_stack);
+    launch_batch(cls, minb_of(grp), grp > 4, S.st, S.d_jobs, S.d_ctl + grp, S.sms, uniform ? &u : nullptr, stack);
   };
   auto kernels = [&](bool all_groups) {
     for (int c = 1; c < RB_GROUPS; ++c)
@@ -638,7 +655,7 @@ static int server_step(Server &S) {
         wj.push_back(w);
       }
       uint64_t c[4] = {0, 0, 0, 0};
-      const int rc = wf_render_jobs(S.scenes[sc], wj.data(), (int)wj.size(), RB_SERVER_WF_QUEUE, c, S.st_wf);
+      const int rc = wf_render_jobs(S.scenes[sc], wj.data(), (int)wj.size(), S.wf_cap, c, S.st_wf);
       if (rc != RB_OK) return rc;
       wf_segments += c[0];
       wf_paths += c[1];
@@ -907,7 +924,8 @@ int rb_server_add_scene(rb_server *r, const rb_cuda_scene *scene) {
   // the wavefront engine's queues and march buffers are allocated when a
   // smooth-SDF scene joins, not inside the first request's iteration
   if (on_wavefront_scene(r->s, ds)) {
-    const int rc = wf_render_jobs(ds, nullptr, 0, RB_SERVER_WF_QUEUE, nullptr, r->s.st);
+    r->s.wf_cap = std::max(r->s.wf_cap, scene_wf_queue(ds));
+    const int rc = wf_render_jobs(ds, nullptr, 0, r->s.wf_cap, nullptr, r->s.st);
     if (rc != RB_OK) return rc;
   }
   r->s.scenes.push_back(ds);
@@ -1172,7 +1190,7 @@ int rb_render_views(const rb_cuda_scene *scene, int n_views, int width, int heig
   uni.S = ds->view;
   uni.G = G;
   launch_batch(ds->ms, minb, G.nee != 0, st, reinterpret_cast<const BatchJob *>(T.d + sizeof(BatchCtl)), d_ctl, sms,
-               &uni);
+               &uni, ds->view.short_stack);
   if (!cuda_ok(cudaGetLastError(), "rb_render_views: launch")) return RB_ERR_CUDA;
   if (counters &&
       !cuda_ok(cudaMemcpyAsync(counters, &d_ctl->segments, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st),

@@ -132,7 +132,8 @@ struct __align__(16) SdfPrim {
   float r11, r12, r20, r21;
   float r22;
   int material;
-  float pad[2];
+  float bound_r;  // the k-inflated bounding-sphere radius (centre px, py, pz)
+  int convex;     // 1: distance convex along a ray (sphere, box, rounded box, capsule)
 };
 static_assert(sizeof(SdfPrim) == 80, "SdfPrim is five 16-byte words");
 
@@ -160,6 +161,7 @@ struct SceneView {
   float sdf_k;         // smooth-union radius
   float sdf_eps;
   int trav_budget;     // traversal step budget override (0: 2 * (prims + 4) + 64)
+  int short_stack;     // traversal stack entries in shared memory (0: RB_SHORT)
   // Rays whose traversal ran out of its step budget (a corrupt tree; never a
   // well-formed one): counted here, read by rb_scene_traversal_faults.
   unsigned long long *faults;
@@ -286,11 +288,47 @@ struct SdfCand {
   int n;
   int idx[RB_SDF_CAND];
   float t0[RB_SDF_CAND], t1[RB_SDF_CAND];
+  // code = SDF table index << 1 | convex flag; window [t0, t1] along the ray
+  __device__ __forceinline__ void add(int code, float a0, float a1) {
+    if (n < RB_SDF_CAND) {
+      idx[n] = code;
+      t0[n] = a0;
+      t1[n] = a1;
+      ++n;
+    }
+  }
 };
 
-template <int MS>
+// The wavefront engine's candidate set: one bit per SDF table entry (tables of
+// at most RB_SDF_MASK_BITS primitives), kept in registers. Index order comes
+// for free (no per-ray arrays, no sort) and the set has no size cap; the
+// march recomputes each window from the primitive's bounding sphere.
+#define RB_SDF_MASK_WORDS 8
+#define RB_SDF_MASK_BITS (32 * RB_SDF_MASK_WORDS)
+struct SdfMask {
+  uint32_t w[RB_SDF_MASK_WORDS];
+  __device__ __forceinline__ void clear() {
+#pragma unroll
+    for (int k = 0; k < RB_SDF_MASK_WORDS; ++k) w[k] = 0u;
+  }
+  __device__ __forceinline__ void add(int code, float, float) {
+    const int i = code >> 1;
+    const uint32_t bit = 1u << (i & 31);
+#pragma unroll
+    for (int k = 0; k < RB_SDF_MASK_WORDS; ++k)
+      if (k == (i >> 5)) w[k] |= bit;  // static indices: the words stay in registers
+  }
+  __device__ __forceinline__ bool any() const {
+    uint32_t a = 0u;
+#pragma unroll
+    for (int k = 0; k < RB_SDF_MASK_WORDS; ++k) a |= w[k];
+    return a != 0u;
+  }
+};
+
+template <int MS, class Sink = SdfCand>
 __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
-                                       float &t, SdfCand *cand = nullptr) {
+                                       float &t, Sink *cand = nullptr) {
   const float4 *p = S.prims + 3 * (size_t)i;
   const float4 a = __ldg(p);
   const float4 c = __ldg(p + 2);
@@ -311,12 +349,7 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
       if (disc >= 0.0f) {
         const float sq = sqrtf(disc);
         const float t0 = (-hb - sq) / aa, t1 = (-hb + sq) / aa;
-        if (t1 >= tmin && t0 <= tmax && cand->n < RB_SDF_CAND) {
-          cand->idx[cand->n] = (__float_as_int(b.x) << 1) | (__float_as_int(b.y) & 1);
-          cand->t0[cand->n] = t0;
-          cand->t1[cand->n] = t1;
-          ++cand->n;
-        }
+        if (t1 >= tmin && t0 <= tmax) cand->add((__float_as_int(b.x) << 1) | (__float_as_int(b.y) & 1), t0, t1);
       }
       return false;
     }
@@ -340,30 +373,61 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
 // sequence of primitive tests, and so the closest-hit result with its
 // equal-t tie rule, is the reference's.
 //
-// Stack: the top RB_SHORT entries live in shared memory (one column per
-// thread, conflict-free), deeper ones in local memory. 32 entries in all; as
-// in the reference a push beyond 32 is dropped (and counted).
+// Stack: the top `nsh` entries live in shared memory (one column per thread,
+// conflict-free), deeper ones in local memory. 32 entries in all; as in the
+// reference a push beyond 32 is dropped (and counted). The shared depth is a
+// per-scene tunable (SceneView::short_stack, the autotuner's knob, RB_SHORT by
+// default); each kernel clamps it to the dynamic shared memory its launch was
+// given (stack_init), so a launch can never index past its allocation.
 #ifndef RB_SHORT
 #define RB_SHORT 8
 #endif
+#define RB_SHORT_MAX 16
 #define RB_STACK 32
 
 struct Stack {
-  int2 *sh;     // shared column base for this thread; stride = blockDim
+  int2 *sh;     // shared column base for this thread; stride = threads per block
   int stride;
-  int2 loc[RB_STACK - RB_SHORT];
+  int nsh;      // entries kept in shared memory
+  int2 loc[RB_STACK];
   int sp;
   __device__ __forceinline__ void push(int ref, float te) {
     const int2 e = make_int2(ref, __float_as_int(te));
-    if (sp < RB_SHORT) sh[sp * stride] = e;
-    else loc[sp - RB_SHORT] = e;
+    if (sp < nsh) sh[sp * stride] = e;
+    else loc[sp - nsh] = e;
     ++sp;
   }
   __device__ __forceinline__ int2 pop() {
     --sp;
-    return sp < RB_SHORT ? sh[sp * stride] : loc[sp - RB_SHORT];
+    return sp < nsh ? sh[sp * stride] : loc[sp - nsh];
   }
 };
+
+// Dynamic shared memory of the running launch (PTX special register).
+__device__ __forceinline__ unsigned dynamic_smem_bytes() {
+  unsigned b;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(b));
+  return b;
+}
+
+// The stack of thread `tid` of a block of `threads`: `want` shared entries
+// (0: RB_SHORT), at most what the launch's dynamic shared memory holds for
+// every thread of the block.
+__device__ __forceinline__ void stack_init(Stack &st, int2 *smem, int tid, int threads, int want) {
+  st.sh = smem + tid;
+  st.stride = threads;
+  const int cap = (int)(dynamic_smem_bytes() / (sizeof(int2) * (unsigned)threads));
+  const int w = want > 0 ? want : RB_SHORT;
+  st.nsh = w < cap ? w : cap;
+  st.sp = 0;
+}
+
+// Dynamic shared memory a launch of `threads` threads provides for a stack of
+// `short_stack` shared entries (0: RB_SHORT).
+__host__ __device__ inline size_t stack_smem_bytes(int short_stack, int threads) {
+  const int w = short_stack > 0 ? (short_stack < RB_SHORT_MAX ? short_stack : RB_SHORT_MAX) : RB_SHORT;
+  return sizeof(int2) * (size_t)w * (size_t)threads;
+}
 
 struct HitInfo {
   float t;
@@ -376,9 +440,9 @@ static __device__ bool sdf_field_march(const SceneView &S, const Ray &r, float t
                                        float &t, f3 &n, int &mat);
 
 // Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
-template <bool ANY, int MS, bool SPEC>
+template <bool ANY, int MS, bool SPEC, class Sink = SdfCand>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
-                                             uint32_t &overflow, SdfCand *cand);
+                                             uint32_t &overflow, Sink *cand);
 
 // Closest (or, with ANY, first) hit including the smooth SDF field. SPEC
 // selects the speculative while-while traversal (render kernels); without it
@@ -409,17 +473,17 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
     }
     return h;
   }
-  return trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, nullptr);
+  return trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, static_cast<SdfCand *>(nullptr));
 }
 
-template <bool ANY, int MS>
+template <bool ANY, int MS, class Sink>
 __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
-                                            uint32_t &overflow, SdfCand *cand);
+                                            uint32_t &overflow, Sink *cand);
 
-template <bool ANY, int MS, bool SPEC>
+template <bool ANY, int MS, bool SPEC, class Sink>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
-                                             uint32_t &overflow, SdfCand *cand) {
-  if (SPEC && S.use_bvh) return trace_ww<ANY, MS>(S, ray, tmin, tmax, st, overflow, cand);
+                                             uint32_t &overflow, Sink *cand) {
+  if (SPEC && S.use_bvh) return trace_ww<ANY, MS, Sink>(S, ray, tmin, tmax, st, overflow, cand);
   HitInfo h;
   h.t = tmax;
   h.prim = -1;
@@ -436,7 +500,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
       const int first = __float_as_int(g0.w), end = first + __float_as_int(g1.w);
       for (int i = first; i < end; ++i) {
         float t;
-        if (prim_t<MS>(S, i, ray, tmin, closest, t, cand)) {
+        if (prim_t<MS, Sink>(S, i, ray, tmin, closest, t, cand)) {
           closest = t;
           h.t = t;
           h.prim = i;
@@ -449,7 +513,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
   if (!S.use_bvh) {
     for (int i = 0; i < S.num_prims; ++i) {
       float t;
-      if (prim_t<MS>(S, i, ray, tmin, closest, t, cand)) {
+      if (prim_t<MS, Sink>(S, i, ray, tmin, closest, t, cand)) {
         closest = t;
         h.t = t;
         h.prim = i;
@@ -471,7 +535,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
       const int first = leaf_first(cur), cnt = leaf_count(cur);
       for (int i = 0; i < cnt; ++i) {
         float t;
-        if (prim_t<MS>(S, first + i, ray, tmin, closest, t, cand)) {
+        if (prim_t<MS, Sink>(S, first + i, ray, tmin, closest, t, cand)) {
           closest = t;
           h.t = t;
           h.prim = first + i;
@@ -602,9 +666,9 @@ __device__ __forceinline__ int pop_next(Stack &st, float closest) {
   return RB_TRAV_DONE;
 }
 
-template <bool ANY, int MS>
+template <bool ANY, int MS, class Sink>
 __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
-                                            uint32_t &overflow, SdfCand *cand) {
+                                            uint32_t &overflow, Sink *cand) {
   HitInfo h;
   h.t = tmax;
   h.prim = -1;
@@ -642,7 +706,7 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
       const int first = leaf_first(leaf), cnt = leaf_count(leaf);
       for (int i = 0; i < cnt; ++i) {
         float t;
-        if (prim_t<MS>(S, first + i, ray, tmin, closest, t, cand)) {
+        if (prim_t<MS, Sink>(S, first + i, ray, tmin, closest, t, cand)) {
           closest = t;
           h.t = t;
           h.prim = first + i;

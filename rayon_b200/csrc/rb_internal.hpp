@@ -74,6 +74,10 @@ struct DeviceScene {
   int ms = 3;
   int layout_kind = 0, layout_leaf = 0;
   float probe_ms = 0.0f;
+  // launch configuration chosen by the autotuner (0: the class defaults)
+  int tuned_minb = 0, tuned_bx = 0, tuned_by = 0;
+  int wf_queue = 0;          // wavefront engine path slots for this scene (0: default)
+  bool tune_cached = false;  // the decision came from the per-(GPU, scene) cache
 };
 
 // FP32 camera frame for the kernels (cast from the FP64 frame, as

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -247,6 +248,8 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
       // convex primitives (their distance is convex along a ray) allow the field march's convex skip
       const bool convex = t == RB_SDF_SPHERE || t == RB_SDF_BOX || t == RB_SDF_ROUND_BOX || t == RB_SDF_CAPSULE;
       put(r, 5, __int_as_float_host(convex ? 1 : 0));
+      q.bound_r = getw(r, 3);
+      q.convex = convex ? 1 : 0;
       L.sdf.push_back(q);
       put(r, 11, __uint_as_float_host(tag_of(g, kind)));
     }
@@ -478,8 +481,7 @@ __global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t 
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   if (x >= P.width || y >= P.height) return;
   Stack st;
-  st.sh = smem + tid;
-  st.stride = blockDim.x * blockDim.y;
+  stack_init(st, smem, tid, blockDim.x * blockDim.y, S.short_stack);
   uint32_t ovf = 0;
   const f3 pc = P.p00 + ((float)x + 0.0f) * P.du + ((float)y + 0.0f) * P.dv;
   Ray r;
@@ -514,8 +516,7 @@ __global__ void __launch_bounds__(256, MINB) k_render(SceneView S, Globals G, Fr
   unsigned long long segs = 0;
   if (work) {
     Stack st;
-    st.sh = smem + tid;
-    st.stride = blockDim.x * blockDim.y;
+    stack_init(st, smem, tid, blockDim.x * blockDim.y, S.short_stack);
     uint32_t ovf = 0;
     // sample slice blockIdx.z of gridDim.z (small frames split their samples
     // so that the launch fills the GPU): slice 0 adds into the pixel's sums,
@@ -728,7 +729,7 @@ FrameF frame_from(const double *fr, int w, int h) {
 
 int launch_primary(const DeviceScene *ds, const FrameF &P, int32_t *ids, float *t, cudaStream_t st) {
   dim3 blk(16, 16), grd((P.width + 15) / 16, (P.height + 15) / 16);
-  const size_t sm = sizeof(int2) * RB_SHORT * blk.x * blk.y;
+  const size_t sm = stack_smem_bytes(ds->view.short_stack, blk.x * blk.y);
   k_primary<<<grd, blk, sm, st>>>(ds->view, P, ids, t);
   g_launches++;
   return cuda_ok(cudaGetLastError(), "k_primary launch") ? RB_OK : RB_ERR_CUDA;
@@ -818,13 +819,21 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   const int ms = ds->ms;
   int bx, by;
   default_block(ms, bx, by);
+  if (ds->tuned_bx > 0 && ds->tuned_by > 0) {
+    bx = ds->tuned_bx;
+    by = ds->tuned_by;
+  }
   if (o.block_x > 0 && o.block_y > 0 && o.block_x * o.block_y <= 256 && o.block_x * o.block_y >= 32) {
     bx = o.block_x;
     by = o.block_y;
   }
   dim3 blk(bx, by), grd((P.width + bx - 1) / bx, (P.height + by - 1) / by);
-  const size_t sm = sizeof(int2) * RB_SHORT * blk.x * blk.y;
-  const int minb = o.reserved[0] > 0 ? o.reserved[0] : default_minb(ms, G.nee != 0);
+  const size_t sm = stack_smem_bytes(ds->view.short_stack, blk.x * blk.y);
+  // register budget: an explicit option, else the scene's tuned one (tuned
+  // without next-event estimation, whose variant needs more registers), else
+  // the class default
+  const int minb = o.reserved[0] > 0 ? o.reserved[0]
+                   : (ds->tuned_minb > 0 && !G.nee) ? ds->tuned_minb : default_minb(ms, G.nee != 0);
   // A frame with fewer pixels than four times the GPU's resident threads
   // splits its samples into up to 8 slices (grid z), so that the launch keeps
   // the GPU full to its end (measured on B200: 400x225 x 32 spp 1.99 -> 1.13 ms,
@@ -959,6 +968,95 @@ static float probe_once(const DeviceScene *ds, const FrameF &P0, cudaStream_t st
   return best;
 }
 
+static float probe_ms(const DeviceScene *ds, const std::vector<FrameF> &frames, cudaStream_t st);
+
+// The scene's k_render launch configuration; the shared stack depth lives in
+// the scene view, so the handle's device copy of the view is refreshed too.
+static void apply_launch_choice(DeviceScene *ds, int minb, int bx, int by, int short_stack, cudaStream_t st) {
+  ds->tuned_minb = minb;
+  ds->tuned_bx = bx;
+  ds->tuned_by = by;
+  ds->view.short_stack = short_stack;
+  cuda_ok(cudaMemcpyAsync(ds->handle, &ds->view, sizeof ds->view, cudaMemcpyHostToDevice, st), "tuned view");
+  cudaStreamSynchronize(st);
+}
+
+// Second stage of the autotuner, on the chosen layout: the per-pixel kernel's
+// register budget (2, 3 or 4 resident 256-thread blocks per SM) and block
+// shape (8x8, 16x8, 16x16, 32x8), then, for BVH layouts, the traversal
+// stack's shared-memory depth (4, 8, 16 entries). Each candidate is timed on
+// the probe frames; the class defaults stay unless a candidate beats them by
+// more than 2 %.
+static void tune_launch(DeviceScene *ds, const std::vector<FrameF> &frames, cudaStream_t st) {
+  int bx0, by0;
+  default_block(ds->ms, bx0, by0);
+  const int minb0 = default_minb(ds->ms, false);
+  apply_launch_choice(ds, minb0, bx0, by0, RB_SHORT, st);
+  float best = probe_ms(ds, frames, st);
+  int bm = minb0, bbx = bx0, bby = by0, bsh = RB_SHORT;
+  const int blocks[4][2] = {{8, 8}, {16, 8}, {16, 16}, {32, 8}};
+  for (int m : {2, 3, 4})
+    for (const auto &b : blocks) {
+      if (m == minb0 && b[0] == bx0 && b[1] == by0) continue;
+      apply_launch_choice(ds, m, b[0], b[1], RB_SHORT, st);
+      const float t = probe_ms(ds, frames, st);
+      if (t < 0.98f * best) {
+        best = t;
+        bm = m;
+        bbx = b[0];
+        bby = b[1];
+      }
+    }
+  if (ds->layout_kind == RB_LAYOUT_LEAF && ds->view.use_bvh)
+    for (int sh : {4, 16}) {
+      apply_launch_choice(ds, bm, bbx, bby, sh, st);
+      const float t = probe_ms(ds, frames, st);
+      if (t < 0.98f * best) {
+        best = t;
+        bsh = sh;
+      }
+    }
+  apply_launch_choice(ds, bm, bbx, bby, bsh, st);
+  ds->probe_ms = best;
+}
+
+// Third stage, for scenes with a smooth SDF field (rendered by the wavefront
+// engine): the engine's path slots (2, 4, 8 or 16 M), timed on a 16.8 M-path
+// probe (the probe view at 256 samples per pixel; more paths than the largest
+// candidate holds, so every candidate regenerates paths as in a real run).
+static int tune_wavefront_queue(DeviceScene *ds, const FrameF &P0, cudaStream_t st) {
+  const int W = P0.width, H = P0.height;
+  double *acc = nullptr;
+  if (!cuda_ok(cudaMalloc(&acc, sizeof(double) * 4 * (size_t)W * H), "wavefront probe buffer")) return 0;
+  WfJob J;
+  std::memset(&J, 0, sizeof J);
+  J.P = P0;
+  J.P.samples = 256;
+  J.P.sample_base = 0;
+  J.G = current_globals();
+  J.G.nee = 0;
+  J.G.dof_enabled = 0;
+  J.acc = acc;
+  int best_cap = 0;
+  double best = 1e30;
+  for (int cap : {1 << 21, 1 << 22, 1 << 23, 1 << 24}) {
+    WfJob j = J;
+    if (wf_render_jobs(ds, &j, 1, cap, nullptr, st) != RB_OK) break;  // also allocates at this capacity
+    j = J;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = wf_render_jobs(ds, &j, 1, cap, nullptr, st);
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc != RB_OK) break;
+    if (s < 0.98 * best) {
+      best = s;
+      best_cap = cap;
+    }
+  }
+  cudaGetLastError();
+  cudaFree(acc);
+  return best_cap;
+}
+
 static std::vector<FrameF> probe_frames(const HostScene &hs, const rb_upload_opts &o, int depth) {
   std::vector<FrameF> out;
   const int W = 256, H = 256;
@@ -1015,6 +1113,9 @@ struct TuneChoice {
   int leaf;    // BVH leaf size
   int groups;  // > 0: grouped linear layout with groups of at most this many primitives
   float probe_ms = 0.0f;  // the probe time that decided it
+  int minb = 0, bx = 0, by = 0;  // k_render register budget and block shape
+  int short_stack = 0;           // traversal stack entries in shared memory
+  int wf_queue = 0;              // wavefront path slots (smooth-SDF scenes)
 };
 static std::unordered_map<TuneKey, TuneChoice, TuneKeyHash> g_tune_cache;
 
@@ -1107,11 +1208,27 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
     set_error("rb_scene_upload: no layout could be uploaded");
     return nullptr;
   }
-  if (!cached) {
+  if (cached) {
+    const TuneChoice &c = cands[0];
+    apply_launch_choice(best, c.minb, c.bx, c.by, c.short_stack, st);
+    best->wf_queue = c.wf_queue;
+    best->tune_cached = true;
+    return best;
+  }
+  tune_launch(best, frames, st);
+  if (best->ms >= RB_MS_SDF && best->view.sdf_k > 0.0f && best->view.num_sdf > 0)
+    best->wf_queue = tune_wavefront_queue(best, frames[0], st);
+  {
     std::lock_guard<std::mutex> lk(g_mu);
     const bool groups = best->layout_kind == RB_LAYOUT_GROUPS;
-    g_tune_cache[key] = {best->layout_kind == RB_LAYOUT_LINEAR, groups ? 0 : best->layout_leaf,
-                         groups ? best->layout_leaf : 0, best->probe_ms};
+    TuneChoice c{best->layout_kind == RB_LAYOUT_LINEAR, groups ? 0 : best->layout_leaf, groups ? best->layout_leaf : 0,
+                 best->probe_ms};
+    c.minb = best->tuned_minb;
+    c.bx = best->tuned_bx;
+    c.by = best->tuned_by;
+    c.short_stack = best->view.short_stack;
+    c.wf_queue = best->wf_queue;
+    g_tune_cache[key] = c;
   }
   return best;
 }
@@ -1396,6 +1513,23 @@ rb_cuda_scene *rb_scene_upload(const rb_scene_desc *s, const rb_upload_opts *opt
     return nullptr;
   }
   return ds ? static_cast<rb_cuda_scene *>(ds->handle) : nullptr;
+}
+
+int rb_scene_tuning(const rb_cuda_scene *scene, rb_tuning *out) {
+  DeviceScene *ds = lookup_scene(scene);
+  if (!ds) return RB_ERR_NOT_FOUND;
+  if (!out) return RB_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof *out);
+  out->layout = ds->layout_kind;
+  out->leaf = ds->layout_leaf;
+  out->blocks_per_sm = ds->tuned_minb;
+  out->block_x = ds->tuned_bx;
+  out->block_y = ds->tuned_by;
+  out->short_stack = ds->view.short_stack;
+  out->wavefront_queue = ds->wf_queue;
+  out->probe_ms = ds->probe_ms;
+  out->from_cache = ds->tune_cached ? 1 : 0;
+  return RB_OK;
 }
 
 int rb_scene_layout_info(const rb_cuda_scene *scene, int *kind, int *leaf, float *probe_ms) {

@@ -124,7 +124,13 @@ __global__ void k_wf_fill(WfParams W, WfQueue q, int qi, int capacity) {
 #ifndef WF_EXTEND_MINB
 #define WF_EXTEND_MINB 4
 #endif
-template <int MS>
+// Candidate sets of the smooth SDF field: RB_SDF_MASK_BITS-bit masks (tables
+// of at most that many primitives; rows 0 and 1 of the candidate buffer hold
+// words 0-3 and 4-7) or, for larger tables, sorted window records.
+#ifndef WF_SDF_MASK
+#define WF_SDF_MASK 1
+#endif
+template <int MS, bool MASK>
 __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(WfParams W, WfQueue q, int qi) {
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -133,14 +139,25 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(WfParams W, W
   bool march = false;
   if (valid) {
     Stack st;
-    st.sh = smem + threadIdx.x;
-    st.stride = blockDim.x;
+    stack_init(st, smem, threadIdx.x, blockDim.x, W.S.short_stack);
     uint32_t ovf = 0;
     const float4 o = q.o[k], d = q.d[k];
     Ray r;
     r.o = f3(o.x, o.y, o.z);
     r.d = f3(d.x, d.y, d.z);
-    if (MS >= RB_MS_SDF && wf_marches(W)) {
+    if (MS >= RB_MS_SDF && MASK && wf_marches(W)) {
+      // traversal only: the field is marched by k_wf_march; the crossed
+      // primitives are kept as a bit set (index order, no per-ray arrays)
+      SdfMask cand;
+      cand.clear();
+      const HitInfo h = trace_bvh<false, MS, RB_SPEC_TRAVERSAL, SdfMask>(W.S, r, 0.001f, FLT_MAX, st, ovf, &cand);
+      q.hit[k] = make_float4(h.t, __int_as_float(h.prim), 0.f, 0.f);
+      if (cand.any()) {
+        W.cand[k] = make_int4((int)cand.w[0], (int)cand.w[1], (int)cand.w[2], (int)cand.w[3]);
+        W.cand[(size_t)W.cap + k] = make_int4((int)cand.w[4], (int)cand.w[5], (int)cand.w[6], (int)cand.w[7]);
+        march = true;
+      }
+    } else if (MS >= RB_MS_SDF && wf_marches(W)) {
       // traversal only: the field is marched by k_wf_march
       SdfCand cand;
       cand.n = 0;
@@ -243,6 +260,102 @@ __device__ __forceinline__ float wf_fold(const SceneView &S, const WfParams &W, 
   return F;
 }
 
+// --- candidate sets as bit masks (tables of at most RB_SDF_MASK_BITS primitives)
+// The window of table entry i along the ray: its k-inflated bounding sphere
+// (centre in word 0, radius in word 4), the same operations as the extend
+// kernel's collection test. false when the ray misses the sphere.
+__device__ __forceinline__ bool wf_window(const float4 *tab, int i, const Ray &r, float aa, float &t0, float &t1) {
+  const float4 w0 = tab[5 * i], w4 = tab[5 * i + 4];
+  const f3 oc = r.o - f3(w0.x, w0.y, w0.z);
+  const float hb = dot(oc, r.d), cc = dot(oc, oc) - w4.z * w4.z;
+  const float disc = hb * hb - aa * cc;
+  if (disc < 0.0f) return false;
+  const float sq = sqrtf(disc);
+  t0 = (-hb - sq) / aa;
+  t1 = (-hb + sq) / aa;
+  return true;
+}
+
+#define WF_MARK_REG 4
+// Marks, in index order, the candidates whose window holds t: the first
+// WF_MARK_REG of them in mid[] (registers), their total in *count; also the
+// next window entry beyond t and the earliest exit among the held windows.
+__device__ __forceinline__ void wf_mark_mask(const float4 *tab, const uint32_t (&cm)[RB_SDF_MASK_WORDS], const Ray &r,
+                                             float t, int (&mid)[WF_MARK_REG], int &count, float &next, float &exit) {
+  const float aa = dot(r.d, r.d);
+  float nx = RB_SDF_FAR, ex = RB_SDF_FAR;
+  int c = 0;
+#pragma unroll
+  for (int w = 0; w < RB_SDF_MASK_WORDS; ++w) {
+    uint32_t m = cm[w];
+    while (m) {
+      const int i = 32 * w + __ffs(m) - 1;
+      m &= m - 1;
+      float t0, t1;
+      if (!wf_window(tab, i, r, aa, t0, t1)) continue;
+      if (t0 > t) {
+        nx = fminf(nx, t0);
+      } else if (t <= t1) {
+#pragma unroll
+        for (int k = 0; k < WF_MARK_REG; ++k)
+          if (k == c) mid[k] = i;
+        ++c;
+        ex = fminf(ex, t1);
+      }
+    }
+  }
+  count = c;
+  next = nx;
+  exit = ex;
+}
+
+// One marked candidate folded into the field at p.
+__device__ __forceinline__ void wf_fold_one(const SceneView &S, const float4 *tab, int i, const f3 &p, float &F,
+                                            bool &first, float &best, int *nearest) {
+  const float d = sdf_eval_words(tab[5 * i], tab[5 * i + 1], tab[5 * i + 2], tab[5 * i + 3], tab[5 * i + 4], p);
+  if (nearest && d < best) {
+    best = d;
+    *nearest = i;
+  }
+  F = first ? d : smin_poly(F, d, S.sdf_k);
+  first = false;
+}
+
+// The field at p over the marked candidates (RB_SDF_FAR when none): the
+// lanes fold their k-th marked candidate together; a ray holding more than
+// WF_MARK_REG windows at t finds the rest again from its candidate mask
+// (indices above mid[WF_MARK_REG - 1], window test at t). `lone` is the
+// candidate code (index << 1 | convex) when exactly one window holds t.
+__device__ __forceinline__ float wf_fold_mask(const SceneView &S, const float4 *tab,
+                                              const uint32_t (&cm)[RB_SDF_MASK_WORDS], const Ray &r, float t,
+                                              const int (&mid)[WF_MARK_REG], int count, const f3 &p, int *nearest,
+                                              int &lone) {
+  float F = RB_SDF_FAR, best = RB_SDF_FAR;
+  bool first = true;
+  lone = -1;
+  const int nreg = count < WF_MARK_REG ? count : WF_MARK_REG;
+#pragma unroll
+  for (int k = 0; k < WF_MARK_REG; ++k)
+    if (k < nreg) wf_fold_one(S, tab, mid[k], p, F, first, best, nearest);
+  if (count == 1) lone = (mid[0] << 1) | (__float_as_int(tab[5 * mid[0] + 4].w) & 1);
+  if (count > WF_MARK_REG) {  // rare: more windows hold t than the registers keep
+    const float aa = dot(r.d, r.d);
+    const int after = mid[WF_MARK_REG - 1];
+#pragma unroll
+    for (int w = 0; w < RB_SDF_MASK_WORDS; ++w) {
+      uint32_t m = cm[w];
+      while (m) {
+        const int i = 32 * w + __ffs(m) - 1;
+        m &= m - 1;
+        float t0, t1;
+        if (i > after && wf_window(tab, i, r, aa, t0, t1) && t0 <= t && t <= t1)
+          wf_fold_one(S, tab, i, p, F, first, best, nearest);
+      }
+    }
+  }
+  return F;
+}
+
 // Persistent field march over the march list. Every pass, each busy lane
 // evaluates the field exactly once, whatever its phase, so the warp's lanes
 // evaluate in lockstep: escape (stepping out of the eps shell, up to 8
@@ -262,7 +375,7 @@ enum : int { WF_ESCAPE = 0, WF_MARCH = 1, WF_NORMAL = 2 };
 #ifndef WF_MARCH_MINB
 #define WF_MARCH_MINB 4
 #endif
-template <int MS>
+template <int MS, bool MASK>
 __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQueue q, int stage_table) {
   extern __shared__ float4 s_tab[];
   const int lane = threadIdx.x & 31;
@@ -284,6 +397,14 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
   int4 cr[WF_CAND_REG];
 #pragma unroll
   for (int i = 0; i < WF_CAND_REG; ++i) cr[i] = make_int4(0, 0, 0, 0);
+  // MASK: the ray's candidate mask and its marked windows (first WF_MARK_REG in registers)
+  uint32_t cm[RB_SDF_MASK_WORDS];
+  int mid[WF_MARK_REG];
+  int mcount = 0;
+#pragma unroll
+  for (int i = 0; i < RB_SDF_MASK_WORDS; ++i) cm[i] = 0u;
+#pragma unroll
+  for (int i = 0; i < WF_MARK_REG; ++i) mid[i] = 0;
   float t = 0.f, tmax = 0.f, sgn = 1.f, inv_len = 1.f;
   f3 p(0.f, 0.f, 0.f), g(0.f, 0.f, 0.f);
   Ray r;
@@ -302,10 +423,16 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
         const unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
         if (idx < total) {
           slot = W.list[idx];
-          n = W.ncand[slot];
+          if constexpr (MASK) {
+            const int4 a = __ldg(W.cand + slot), b = __ldg(W.cand + (size_t)W.cap + slot);
+            cm[0] = (uint32_t)a.x; cm[1] = (uint32_t)a.y; cm[2] = (uint32_t)a.z; cm[3] = (uint32_t)a.w;
+            cm[4] = (uint32_t)b.x; cm[5] = (uint32_t)b.y; cm[6] = (uint32_t)b.z; cm[7] = (uint32_t)b.w;
+          } else {
+            n = W.ncand[slot];
 #pragma unroll
-          for (int i = 0; i < WF_CAND_REG; ++i)
-            if (i < n) cr[i] = __ldg(W.cand + (size_t)i * W.cap + slot);
+            for (int i = 0; i < WF_CAND_REG; ++i)
+              if (i < n) cr[i] = __ldg(W.cand + (size_t)i * W.cap + slot);
+          }
           const float4 o = q.o[slot], d = q.d[slot];
           r.o = f3(o.x, o.y, o.z);
           r.d = f3(d.x, d.y, d.z);
@@ -334,10 +461,18 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
     } else {
       pe = r.at(t);
     }
-    if (!(t < mark_next && t <= mark_exit)) wf_mark(W, cr, slot, n, t, marked, mark_next, mark_exit);
+    int near, lone;
+    float raw;
+    if constexpr (MASK) {
+      if (!(t < mark_next && t <= mark_exit)) wf_mark_mask(tab, cm, r, t, mid, mcount, mark_next, mark_exit);
+      near = mid[0];
+      raw = wf_fold_mask(S, tab, cm, r, t, mid, mcount, pe, phase == WF_NORMAL ? nullptr : &near, lone);
+    } else {
+      if (!(t < mark_next && t <= mark_exit)) wf_mark(W, cr, slot, n, t, marked, mark_next, mark_exit);
+      near = cr[0].x >> 1;
+      raw = wf_fold(S, W, tab, slot, cr, marked, pe, phase == WF_NORMAL ? nullptr : &near, lone);
+    }
     const float next = mark_next;
-    int near = cr[0].x >> 1, lone;
-    const float raw = wf_fold(S, W, tab, slot, cr, marked, pe, phase == WF_NORMAL ? nullptr : &near, lone);
     bool finished = false;
     if (phase == WF_NORMAL) {
       if (sub & 1) {
@@ -421,8 +556,7 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
   bool regenerate = false;
   if (k < n_in) {
     Stack st;
-    st.sh = smem + threadIdx.x;
-    st.stride = blockDim.x;
+    stack_init(st, smem, threadIdx.x, blockDim.x, W.S.short_stack);
     uint32_t ovf = 0;
     const float4 o = in.o[k], d = in.d[k], th = in.thr[k], Lv = in.L[k], hv = in.hit[k];
     const int4 m = in.meta[k];
@@ -599,13 +733,18 @@ struct WfEngine {
   cudaEvent_t fence = nullptr;
 };
 
+// Frees everything the engine holds and nulls the pointers, so that a second
+// call (after a failed allocation) frees nothing twice.
 static void wf_free(WfEngine &E) {
   for (int i = 0; i < 2; ++i) {
     cudaFree(E.q[i].o); cudaFree(E.q[i].d); cudaFree(E.q[i].thr); cudaFree(E.q[i].L);
     cudaFree(E.q[i].hit); cudaFree(E.q[i].sn); cudaFree(E.q[i].meta);
   }
+  std::memset(&E.q, 0, sizeof E.q);
   cudaFree(E.ctl);
   cudaFreeHost(E.h_ctl);
+  E.ctl = nullptr;
+  E.h_ctl = nullptr;
   cudaFree(E.cand);
   cudaFree(E.ncand);
   cudaFree(E.list);
@@ -657,14 +796,24 @@ static size_t wf_table_bytes(const WfParams &W) {
   return b <= 48 * 1024 ? b : 0;
 }
 
+// Candidate sets as bit masks when the field's table fits the mask and is
+// staged in shared memory (the march reads each window's sphere from it).
+static bool wf_use_mask(const WfParams &W) {
+  return WF_SDF_MASK && WF_STAGE_SDF_TABLE && W.cand && W.S.num_sdf > 0 && W.S.num_sdf <= RB_SDF_MASK_BITS &&
+         wf_table_bytes(W) > 0;
+}
+
 template <int MS, bool NEE>
 static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int march_grid, cudaStream_t st) {
-  const size_t sm = sizeof(int2) * RB_SHORT * 256;
+  const size_t sm = stack_smem_bytes(W.S.short_stack, 256);
+  const bool mask = wf_use_mask(W);
   k_wf_reset<<<1, 1, 0, st>>>(E.ctl, qi ^ 1);
-  k_wf_extend<MS><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
+  if (mask) k_wf_extend<MS, true><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
+  else k_wf_extend<MS, false><<<grid, 256, sm, st>>>(W, E.q[qi], qi);
   if (march_grid > 0) {
     const size_t tab = WF_STAGE_SDF_TABLE ? wf_table_bytes(W) : 0;
-    k_wf_march<MS><<<march_grid, 256, tab, st>>>(W, E.q[qi], tab > 0 ? 1 : 0);
+    if (mask) k_wf_march<MS, true><<<march_grid, 256, tab, st>>>(W, E.q[qi], 1);
+    else k_wf_march<MS, false><<<march_grid, 256, tab, st>>>(W, E.q[qi], tab > 0 ? 1 : 0);
   }
   k_wf_shade<MS, NEE><<<grid, 256, sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
 }
@@ -675,8 +824,11 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   int march_grid = 0;
   if (MS >= RB_MS_SDF && W.cand) {  // persistent march: the resident blocks
     int per_sm = 0, dev = 0, sms = 148;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS>, 256,
-                                                  WF_STAGE_SDF_TABLE ? wf_table_bytes(W) : 0);
+    if (wf_use_mask(W))
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS, true>, 256, wf_table_bytes(W));
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_march<MS, false>, 256,
+                                                    WF_STAGE_SDF_TABLE ? wf_table_bytes(W) : 0);
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     march_grid = std::max(1, per_sm) * sms;
@@ -742,7 +894,7 @@ int wf_render_jobs(const DeviceScene *ds, WfJob *jobs, int njobs, int queue_capa
   if (!priv[dev] && !cuda_ok(cudaStreamCreateWithFlags(&priv[dev], cudaStreamNonBlocking), "wavefront stream"))
     return RB_ERR_CUDA;
   cudaStream_t st = priv[dev];
-  const int cap = queue_capacity > 0 ? queue_capacity : (1 << 20);
+  const int cap = queue_capacity > 0 ? queue_capacity : ds->wf_queue > 0 ? ds->wf_queue : (1 << 20);
   WfEngine &E = cached[dev];
   if (E.capacity != cap) {
     if (E.capacity) wf_free(E);

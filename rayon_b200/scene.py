@@ -261,6 +261,14 @@ class DeviceScene:
         kind = {2: "linear", 4: "groups"}.get(k.value, "bvh")
         return {"kind": kind, "leaf": leaf.value, "probe_ms": ms.value}
 
+    @property
+    def tuning(self) -> dict:
+        """The autotuner's decision for this scene (rb_tuning)."""
+        from ._native import Tuning
+        t = Tuning()
+        check(lib.rb_scene_tuning(self.handle, C.byref(t)), "rb_scene_tuning")
+        return {f: getattr(t, f) for f, _ in Tuning._fields_ if f != "reserved_"}
+
     def traversal_faults(self, reset: bool = False) -> int:
         """Rays whose BVH traversal ran out of its step budget (0 for a well-formed tree)."""
         n = C.c_uint64(0)

@@ -42,6 +42,16 @@ def _free_port():
     return p
 
 
+def _fake_range(first, count, npx):
+    """A stand-in for one rank's render of samples [first, first + count):
+    sample s adds pixel % 7 + 0.5 s to every channel (exact in FP32)."""
+    pix = torch.arange(npx, dtype=torch.float32)
+    acc = torch.zeros((2, npx, 4), dtype=torch.float32)
+    for s in range(first, first + count):
+        acc[0, :, :3] += (pix % 7 + 0.5 * s)[:, None]
+    return acc
+
+
 def _worker(rank, world, port, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -59,7 +69,20 @@ def _worker(rank, world, port, q):
         shard = multigpu.shard_jobs(costs, world)[rank]
         res = multigpu.gather_results({i: np.full(3, i, np.float32) for i in shard})
         ok_gather = sorted(res) == list(range(10)) and all(float(res[i][0]) == i for i in res)
-        q.put((rank, ok_reduce, ok_gather))
+        # sample split: each rank renders only its range; the reduce gives the
+        # single-process sums of all samples (values exact in FP32)
+        spp, npx = 37, 50
+        total = multigpu.render_sample_split(lambda f, c: _fake_range(f, c, npx), spp)
+        ok_split = torch.equal(total, _fake_range(0, spp, npx)[0, :, :3].double())
+        # sharded serving: every job served once, stats gathered on every rank
+        jc = [float(c) for c in (5, 1, 9, 3, 7, 2, 8)]
+        out = multigpu.serve_sharded(jc, lambda idx: {"latencies": {i: 0.5 * i for i in idx},
+                                                      "paths": int(sum(jc[i] for i in idx)),
+                                                      "seconds": 1.0 + rank})
+        ok_serve = (sorted(out["latencies"]) == list(range(len(jc))) and
+                    sorted(i for sh in out["shards"] for i in sh) == list(range(len(jc))) and
+                    sum(out["paths"]) == int(sum(jc)) and abs(out["mpaths_s"] - sum(jc) / world / 1e6) < 1e-12)
+        q.put((rank, ok_reduce, ok_gather and ok_split and ok_serve))
     finally:
         dist.destroy_process_group()
 
