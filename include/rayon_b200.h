@@ -423,7 +423,10 @@ typedef struct rb_server_opts {
                                    [2^18, paths_per_iteration], the rule of the progressive
                                    renderer's batch controller (renderer_cuda_progressive_host.hpp:
                                    677-685) applied to the server's quantum. 0: fixed quantum */
-  int reserved[1];
+  int per_frame_classes;        /* bit c set: planned jobs of material class c (1 diffuse, 2 classic,
+                                   3 full, 4 SDF without a smooth field) with FP32 accumulation run
+                                   on the per-frame kernel, one launch per job and iteration over the
+                                   job's planned sample range, instead of the batched kernel */
 } rb_server_opts;
 
 void rb_server_default_opts(rb_server_opts *out);

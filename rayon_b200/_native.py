@@ -191,7 +191,7 @@ class ServerOpts(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_int64), ("max_active_jobs", C.c_int), ("paths_per_iteration", C.c_int64),
                 ("max_spp_per_iteration", C.c_int), ("use_graph", C.c_int), ("frames_every", C.c_int),
                 ("occupancy", C.c_int), ("wavefront_field", C.c_int), ("target_iteration_ms", C.c_float),
-                ("reserved", C.c_int * 1)]
+                ("per_frame_classes", C.c_int)]
 
 
 class JobStatus(C.Structure):

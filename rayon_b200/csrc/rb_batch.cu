@@ -346,6 +346,7 @@ struct Server {
   BatchCtl *h_ctl = nullptr;   // pinned
   BatchCtl *d_ctl = nullptr;
   unsigned long long *h_conv = nullptr, *d_conv = nullptr;  // converged-pixel counts per planned job
+  unsigned long long *h_pfc = nullptr, *d_pfc = nullptr;    // per-frame launches' counters of an iteration
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // wavefront jobs run on their own stream beside the class kernels: ev_up
   // marks the iteration's uploads, ev_wf the end of its wavefront runs
@@ -510,7 +511,8 @@ static int server_step(Server &S) {
   // job gets as many samples per pixel as fit (capped), so tasks are long and
   // an iteration holds few scenes.
   const double tnow = S.now();
-  struct Plan { int64_t id; int spp; int cls; double prio; };
+  // pf: the job runs on the per-frame kernel (rb_server_opts.per_frame_classes)
+  struct Plan { int64_t id; int spp; int cls; double prio; int pf; };
   std::vector<Plan> cand;
   for (int64_t id : S.active) {
     Job &J = S.jobs[id];
@@ -518,7 +520,9 @@ static int server_step(Server &S) {
     const double age = tnow - J.t_arrival;
     // group key: kernel class, plus 4 when the job uses next-event estimation
     const int cls = on_wavefront(S, J) ? RB_WF_GROUP : S.scenes[J.req.scene]->ms + (J.req.nee ? 4 : 0);
-    cand.push_back({id, 0, cls, rem / (1.0 + S.aging * age)});
+    const int ms_cls = cls > 4 ? cls - 4 : cls;
+    const int pf = cls != RB_WF_GROUP && ((S.o.per_frame_classes >> ms_cls) & 1) && J.acc && !J.acc64 ? 1 : 0;
+    cand.push_back({id, 0, cls, rem / (1.0 + S.aging * age), pf});
   }
   std::stable_sort(cand.begin(), cand.end(), [](const Plan &a, const Plan &b) { return a.prio < b.prio; });
   int64_t budget = S.quantum > 0 ? S.quantum : S.o.paths_per_iteration;
@@ -537,19 +541,23 @@ static int server_step(Server &S) {
   // group by kernel class (each class runs its own specialised persistent
   // kernel, so a job's code and results do not depend on the mix); within a
   // class, more samples per task first
+  // per-frame jobs last, so every batched class's tasks stay contiguous
   std::stable_sort(plan.begin(), plan.end(), [](const Plan &a, const Plan &b) {
-    return a.cls != b.cls ? a.cls < b.cls : a.spp > b.spp;
+    return a.pf != b.pf ? a.pf < b.pf : a.cls != b.cls ? a.cls < b.cls : a.spp > b.spp;
   });
   long long tb = 0;
   std::memset(S.h_ctl, 0, sizeof(BatchCtl) * RB_GROUPS);
   int jfirst[RB_GROUPS] = {0};
   std::vector<size_t> wf_k;  // planned jobs that run on the wavefront engine (sorted last)
+  std::vector<size_t> pf_k;  // planned jobs that run on the per-frame kernel
   for (size_t k = 0; k < plan.size(); ++k) {
     Job &J = S.jobs[plan[k].id];
     const DeviceScene *ds = S.scenes[J.req.scene];
     const int cls = plan[k].cls;
     if (cls == RB_WF_GROUP) {
       wf_k.push_back(k);
+    } else if (plan[k].pf) {
+      pf_k.push_back(k);
     } else {
       BatchCtl &C = S.h_ctl[cls];
       if (C.njobs == 0) {
@@ -583,7 +591,7 @@ static int server_step(Server &S) {
                                                      B.spp_total >= J.req.spp);
     B.frame = frame_now ? J.frame : nullptr;
     tb += (long long)J.req.width * J.req.height;
-    if (cls != RB_WF_GROUP) S.h_ctl[cls].total_tasks = (unsigned long long)tb;
+    if (cls != RB_WF_GROUP && !plan[k].pf) S.h_ctl[cls].total_tasks = (unsigned long long)tb;
   }
   for (int c = 1; c < RB_GROUPS; ++c) S.h_ctl[c].job_offset = jfirst[c];
   // groups whose jobs share one scene and one setting run the uniform kernel
@@ -663,7 +671,17 @@ static int server_step(Server &S) {
     return RB_OK;
   };
   const long long frame_blocks_cap = (S.o.paths_per_iteration + 255) / 256 + 1;
-  if (S.o.use_graph && wf_k.empty() && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
+  auto run_per_frame = [&]() -> int {
+    for (size_t k : pf_k) {
+      const Job &J = S.jobs[plan[k].id];
+      const BatchJob &B = S.h_jobs[k];
+      const int n = J.req.width * J.req.height;
+      const int rc = launch_render(S.scenes[J.req.scene], B.G, B.P, J.acc, J.acc + n, nullptr, S.d_pfc, S.st);
+      if (rc != RB_OK) return rc;
+    }
+    return RB_OK;
+  };
+  if (S.o.use_graph && wf_k.empty() && pf_k.empty() && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
     // One graph, reused every iteration: table and control blocks are copied
     // from pinned staging when the graph runs, the three class kernels are
     // persistent (grid = resident blocks) and exit at once when their class
@@ -698,7 +716,13 @@ static int server_step(Server &S) {
     cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
     cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
     cudaEventRecord(S.ev_up, S.st);
+    if (!pf_k.empty()) cudaMemsetAsync(S.d_pfc, 0, sizeof(unsigned long long) * 4, S.st);
     kernels(false);
+    if (!pf_k.empty()) {
+      const int rc = run_per_frame();
+      if (rc != RB_OK) return rc;
+      cudaMemcpyAsync(S.h_pfc, S.d_pfc, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, S.st);
+    }
     if (!wf_k.empty()) {
       // the wavefront jobs touch only their own sums, so they start after the
       // uploads and run beside the class kernels (their blocks take the SMs
@@ -735,6 +759,10 @@ static int server_step(Server &S) {
   }
   S.stats.paths += (int64_t)wf_paths;
   S.stats.segments += (int64_t)wf_segments;
+  if (!pf_k.empty()) {
+    S.stats.segments += (int64_t)S.h_pfc[0];
+    S.stats.paths += (int64_t)S.h_pfc[1];
+  }
   if (frames) S.stats.frames += (int64_t)plan.size();
   // per-job convergence of the jobs that asked for it
   {
@@ -846,7 +874,9 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
             cuda_ok(cudaMallocHost(&S.h_ctl, sizeof(BatchCtl) * RB_GROUPS), "server pinned ctl") &&
             cuda_ok(cudaMalloc(&S.d_ctl, sizeof(BatchCtl) * RB_GROUPS), "server ctl") &&
             cuda_ok(cudaMallocHost(&S.h_conv, sizeof(unsigned long long) * S.o.max_active_jobs), "server conv") &&
-            cuda_ok(cudaMalloc(&S.d_conv, sizeof(unsigned long long) * S.o.max_active_jobs), "server conv");
+            cuda_ok(cudaMalloc(&S.d_conv, sizeof(unsigned long long) * S.o.max_active_jobs), "server conv") &&
+            cuda_ok(cudaMallocHost(&S.h_pfc, sizeof(unsigned long long) * 4), "server per-frame counters") &&
+            cuda_ok(cudaMalloc(&S.d_pfc, sizeof(unsigned long long) * 4), "server per-frame counters");
   if (!ok) {
     rb_server_destroy(r);
     return nullptr;
@@ -898,6 +928,8 @@ void rb_server_destroy(rb_server *r) {
   if (S.d_ctl) cudaFree(S.d_ctl);
   if (S.h_conv) cudaFreeHost(S.h_conv);
   if (S.d_conv) cudaFree(S.d_conv);
+  if (S.h_pfc) cudaFreeHost(S.h_pfc);
+  if (S.d_pfc) cudaFree(S.d_pfc);
   if (S.ev0) cudaEventDestroy(S.ev0);
   if (S.ev1) cudaEventDestroy(S.ev1);
   if (S.st_wf) {

@@ -120,6 +120,9 @@ bool injected_alloc_failure(int site);
 DeviceScene *lookup_scene(const void *handle);
 void build_quantized(HostLayout &L);
 FrameF frame_from(const double *fr, int w, int h);
+// The per-frame kernel over one frame's sample range (rb_render.cu).
+int launch_render(const DeviceScene *ds, const rbd::Globals &G, const FrameF &P, float4 *acc, float4 *comp,
+                  int *counts, unsigned long long *counters, cudaStream_t st);
 struct HostScene;
 rbd::Globals current_globals();
 rb_render_opts current_opts();

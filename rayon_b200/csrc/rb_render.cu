@@ -474,7 +474,8 @@ void unregister_and_free(DeviceScene *ds) {
 // Kernels
 // ---------------------------------------------------------------------------
 // Primary hits through pixel centres (offsets 0 in render_acc_kernel.cu:200-214).
-__global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t *ids, float *tout) {
+__global__ void __launch_bounds__(256) k_primary(const RB_GRID_CONST SceneView S,
+                                                    const RB_GRID_CONST FrameF P, int32_t *ids, float *tout) {
   extern __shared__ int2 smem[];
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -498,7 +499,9 @@ __global__ void __launch_bounds__(256) k_primary(SceneView S, FrameF P, int32_t 
 // per iteration), so a lane whose path ended starts its next sample at once
 // instead of idling until the warp's longest path finishes.
 template <bool NEE, int MS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_render(SceneView S, Globals G, FrameF P, float4 *__restrict__ acc,
+__global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneView S,
+                                                      const RB_GRID_CONST Globals G,
+                                                      const RB_GRID_CONST FrameF P, float4 *__restrict__ acc,
                                                 float4 *__restrict__ comp, float4 *__restrict__ part,
                                                 int *__restrict__ counts, unsigned long long *__restrict__ counters) {
   extern __shared__ int2 smem[];
@@ -1159,7 +1162,9 @@ DeviceScene *autotune_upload(const HostScene &hs, const rb_upload_opts &o0, cuda
         for (int G : {8, 16}) cands.push_back({false, 0, G});
     }
     if (n > 0) {
-      if (n > (1u << 20)) cands.push_back({false, 1, 0}), cands.push_back({false, 4, 0});
+      // large scenes keep the tree they were built with (a rebuild costs seconds)
+      // and tune only the launch configuration
+      if (n > (1u << 20)) cands.push_back({false, hs.use_bvh && !hs.nodes.empty() ? hs.max_leaf : 4, 0});
       else for (int L : {1, 2, 4, 8}) cands.push_back({false, L, 0});
     }
   }

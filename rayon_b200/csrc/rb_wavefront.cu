@@ -107,7 +107,8 @@ __device__ __forceinline__ void wf_emit_camera(const WfParams &W, const WfQueue 
 }
 
 // Initial fill of queue `qi` with min(capacity, total) fresh paths.
-__global__ void k_wf_fill(WfParams W, WfQueue q, int qi, int capacity) {
+__global__ void k_wf_fill(const RB_GRID_CONST WfParams W, const RB_GRID_CONST WfQueue q, int qi,
+                          int capacity) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned long long total = W.ctl->total_paths;
   const unsigned long long n = total < (unsigned long long)capacity ? total : (unsigned long long)capacity;
@@ -131,7 +132,8 @@ __global__ void k_wf_fill(WfParams W, WfQueue q, int qi, int capacity) {
 #define WF_SDF_MASK 1
 #endif
 template <int MS, bool MASK>
-__global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(WfParams W, WfQueue q, int qi) {
+__global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID_CONST WfParams W,
+                                                                   const RB_GRID_CONST WfQueue q, int qi) {
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;

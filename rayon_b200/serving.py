@@ -31,7 +31,8 @@ def job(scene: int, frame, width: int, height: int, spp: int, depth: int, backgr
 class Server:
     def __init__(self, budget_bytes: int | None = None, max_jobs: int | None = None, paths_per_iteration=None,
                  max_spp_per_iteration=None, use_graph: bool = True, frames_every: int = 0, occupancy: int = 0,
-                 wavefront_field: bool = True, target_iteration_ms: float = 0.0, stream=None):
+                 wavefront_field: bool = True, target_iteration_ms: float = 0.0, stream=None,
+                 per_frame_classes: int | None = None):
         o = ServerOpts()
         lib.rb_server_default_opts(C.byref(o))
         if budget_bytes is not None:
@@ -45,6 +46,8 @@ class Server:
         o.use_graph, o.frames_every, o.occupancy = int(use_graph), int(frames_every), int(occupancy)
         o.wavefront_field = int(wavefront_field)
         o.target_iteration_ms = float(target_iteration_ms)
+        if per_frame_classes is not None:
+            o.per_frame_classes = int(per_frame_classes)
         self.h = lib.rb_server_create(C.byref(o), stream)
         if not self.h:
             raise RuntimeError(lib.rb_last_error().decode())

@@ -40,9 +40,12 @@ def _jobs(server_ids, specs):
     return reqs
 
 
-def test_same_alone_and_in_mix(cuda):
+# per_frame_classes: 0 = every class on the batched kernel; 6 = diffuse and
+# classic jobs on the per-frame kernel (one launch per job and iteration)
+@pytest.mark.parametrize("pfc", [0, 6])
+def test_same_alone_and_in_mix(cuda, pfc):
     S = _scenes()
-    mix = serving.Server(paths_per_iteration=200_000, max_spp_per_iteration=16)
+    mix = serving.Server(paths_per_iteration=200_000, max_spp_per_iteration=16, per_frame_classes=pfc)
     ids = [mix.add_scene(ds) for _, _, ds in S]
     reqs = _jobs(ids, S)
     jids = [mix.submit(r) for r, *_ in reqs]
@@ -51,7 +54,7 @@ def test_same_alone_and_in_mix(cuda):
         st = mix.status(jid)
         assert st.state == 2 and st.spp_done == spp
         got = mix.fetch(jid, w, h)
-        alone = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=64)
+        alone = serving.Server(paths_per_iteration=1 << 26, max_spp_per_iteration=64, per_frame_classes=pfc)
         aid = [alone.add_scene(ds) for _, _, ds in S]
         r.scene = aid[r.scene]
         a = alone.submit(r)
@@ -93,12 +96,13 @@ def test_shared_and_per_job_scene_kernels_agree(cuda):
     ds_b.free()
 
 
-def test_server_matches_per_frame_kernel(cuda):
+@pytest.mark.parametrize("pfc", [0, 6])
+def test_server_matches_per_frame_kernel(cuda, pfc):
     spec = scenes.cornell(width=64, height=64)
     sc = spec.to_scene()
     sc.build_bvh()
     ds = sc.upload()
-    srv = serving.Server(paths_per_iteration=64 * 64 * 8)
+    srv = serving.Server(paths_per_iteration=64 * 64 * 8, per_frame_classes=pfc)
     sid = srv.add_scene(ds)
     fr = spec.camera.frame(64, 64)
     j = srv.submit(serving.job(sid, fr, 64, 64, 32, spec.depth, background=0.0, seed=0))
