@@ -1,8 +1,9 @@
 // 8-bit quantised BVH nodes with outward rounding.
 //
-// Each interior node stores its children's boxes on a per-axis power-of-two
-// grid anchored at the union box's minimum corner. Decoding on the device is
-// origin + q * 2^e in FP32; q * 2^e is exact, so the decoded bound is one
+// Each interior node (32 B, one sector) stores its children's boxes on a
+// per-axis power-of-two grid anchored at the union box's minimum corner, the
+// corner kept to 24 bits and rounded toward -inf. Decoding on the device is
+// corner + q * 2^e in FP32; q * 2^e is exact, so the decoded bound is one
 // rounded addition, which this file evaluates the same way and nudges q until
 // min bounds decode <= the FP32 bound and max bounds decode >= it. The decoded
 // box therefore contains the FP32 box, and because rounded subtraction and
@@ -18,29 +19,33 @@ namespace rb {
 
 namespace {
 
+uint32_t f2u(float f) {
+  uint32_t b;
+  std::memcpy(&b, &f, 4);
+  return b;
+}
+float u2f(uint32_t b) {
+  float f;
+  std::memcpy(&f, &b, 4);
+  return f;
+}
+
 float decode(float origin, int q, float scale) {
   volatile float prod = (float)q * scale;  // exact: q < 256, scale a power of two
   volatile float sum = origin + prod;      // one rounding, as on the device
   return sum;
 }
 
-int exponent_for(float extent) {
-  // smallest e with 255 * 2^e >= extent (biased exponent byte, 1..254)
-  if (!(extent > 0.0f)) return 1;
-  int e = (int)std::ceil(std::log2((double)extent / 255.0));
-  while (std::ldexp(255.0, e) < (double)extent) ++e;
-  int biased = e + 127;
-  if (biased < 1) biased = 1;
-  if (biased > 254) biased = 254;
-  return biased;
+// The grid corner kept in a node: the coordinate's FP32 bits with the low 8
+// mantissa bits dropped, rounded toward -inf (never above the coordinate).
+float corner_of(float o) {
+  uint32_t b = f2u(o);
+  if (b & 0xFFu) b = (b & 0x80000000u) ? (b & ~0xFFu) + 0x100u : (b & ~0xFFu);
+  return u2f(b);
 }
 
-float scale_of(int biased) {
-  uint32_t bits = (uint32_t)biased << 23;
-  float f;
-  std::memcpy(&f, &bits, 4);
-  return f;
-}
+// Step 2^e stored as e + 64 in 7 bits (e in [-64, 63]).
+float step_of(int e) { return u2f((uint32_t)(e + 127) << 23); }
 
 }  // namespace
 
@@ -55,30 +60,34 @@ void build_quantized(HostLayout &L) {
       lo[0][k] = w[k]; hi[0][k] = w[3 + k];
       lo[1][k] = w[6 + k]; hi[1][k] = w[9 + k];
     }
-    rbd::QNode q;
-    std::memset(&q, 0, sizeof q);
-    float origin[3];
+    float corner[3], sc[3];
     int ex[3];
-    float sc[3];
     for (int k = 0; k < 3; ++k) {
-      origin[k] = std::fmin(lo[0][k], lo[1][k]);
+      corner[k] = corner_of(std::fmin(lo[0][k], lo[1][k]));
       const float top = std::fmax(hi[0][k], hi[1][k]);
-      ex[k] = exponent_for((float)((double)top - (double)origin[k]) * 1.0001f);
-      sc[k] = scale_of(ex[k]);
+      const double extent = ((double)top - (double)corner[k]) * 1.0001;
+      int e = extent > 0.0 ? (int)std::ceil(std::log2(extent / 255.0)) : -64;
+      e = e < -64 ? -64 : (e > 63 ? 63 : e);
+      while (e < 63 && std::ldexp(255.0, e) < extent) ++e;
       // make sure the whole range is reachable after rounding
-      while (decode(origin[k], 255, sc[k]) < top && ex[k] < 254) sc[k] = scale_of(++ex[k]);
+      while (e < 63 && decode(corner[k], 255, step_of(e)) < top) ++e;
+      ex[k] = e;
+      sc[k] = step_of(e);
     }
-    q.ox = origin[0]; q.oy = origin[1]; q.oz = origin[2];
-    q.meta = (uint32_t)ex[0] | ((uint32_t)ex[1] << 8) | ((uint32_t)ex[2] << 16) | ((uint32_t)wi[2] << 24);
+    const uint32_t axis = (uint32_t)wi[2] & 3u;
+    rbd::QNode q;
+    q.ox = (f2u(corner[0]) & 0xFFFFFF00u) | ((uint32_t)(ex[0] + 64) << 1) | (axis & 1u);
+    q.oy = (f2u(corner[1]) & 0xFFFFFF00u) | ((uint32_t)(ex[1] + 64) << 1) | (axis >> 1);
+    q.oz = (f2u(corner[2]) & 0xFFFFFF00u) | ((uint32_t)(ex[2] + 64) << 1);
     uint8_t b[2][6];
     for (int c = 0; c < 2; ++c)
       for (int k = 0; k < 3; ++k) {
-        int ql = (int)std::floor(((double)lo[c][k] - (double)origin[k]) / (double)sc[k]);
+        int ql = (int)std::floor(((double)lo[c][k] - (double)corner[k]) / (double)sc[k]);
         ql = ql < 0 ? 0 : (ql > 255 ? 255 : ql);
-        while (ql > 0 && decode(origin[k], ql, sc[k]) > lo[c][k]) --ql;
-        int qh = (int)std::ceil(((double)hi[c][k] - (double)origin[k]) / (double)sc[k]);
+        while (ql > 0 && decode(corner[k], ql, sc[k]) > lo[c][k]) --ql;
+        int qh = (int)std::ceil(((double)hi[c][k] - (double)corner[k]) / (double)sc[k]);
         qh = qh < 0 ? 0 : (qh > 255 ? 255 : qh);
-        while (qh < 255 && decode(origin[k], qh, sc[k]) < hi[c][k]) ++qh;
+        while (qh < 255 && decode(corner[k], qh, sc[k]) < hi[c][k]) ++qh;
         b[c][k] = (uint8_t)ql;
         b[c][3 + k] = (uint8_t)qh;
       }

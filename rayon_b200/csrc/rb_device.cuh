@@ -74,20 +74,36 @@ __host__ __forceinline__ int make_leaf_ref(int first, int count) {
   return (int)(0x80000000u | ((uint32_t)(count - 1) << 26) | (uint32_t)first);
 }
 
-// Quantised node (48 B, 3 x 16 B loads): the union box's minimum corner and
-// per-axis power-of-two scales, then 8-bit child bounds rounded outward (min
-// down, max up) so the decoded box always contains the FP32 child box.
-//   f0 = (origin xyz, meta: exponent bytes x, y, z and the split axis)
-//   f1 = (L lo xyz + L hi x, L hi yz + R lo xy, R lo z + R hi xyz, left ref)
-//   f2 = (right ref, 0, 0, 0)
-struct QNode {
-  float ox, oy, oz;
-  uint32_t meta;
+// Quantised node: 32 B, one 32-byte sector per visit (the FP32 two-box node
+// is 64 B, two sectors). A grid anchored at the union box's minimum corner,
+// with a power-of-two step per axis, holds 8-bit child bounds rounded outward
+// (min down, max up), so the decoded box always contains the FP32 child box.
+//   ox, oy, oz: bits 31-8 = the corner coordinate's FP32 bits with the low 8
+//               mantissa bits dropped, rounded toward -inf; bits 7-1 = the
+//               axis's step exponent + 64; bit 0 of ox, oy = the split axis
+//   lq0 = L lo xyz, L hi x;  lq1 = L hi yz, R lo xy;  rq = R lo z, R hi xyz
+//   left, right: child refs
+struct __align__(16) QNode {
+  uint32_t ox, oy, oz;
   uint32_t lq0, lq1, rq;
   int left;
   int right;
-  int pad[3];
 };
+static_assert(sizeof(QNode) == 32, "a quantised node is one 32-byte sector");
+
+// The grid corner and step of one axis word of a quantised node.
+__device__ __host__ __forceinline__ float qnode_origin(uint32_t w) {
+  const uint32_t b = w & 0xFFFFFF00u;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+__device__ __host__ __forceinline__ float qnode_step(uint32_t w) {
+  const uint32_t b = (((w >> 1) & 0x7Fu) + 63u) << 23;  // 2^(stored - 64)
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
 
 // Legacy material kinds of the reference shader (cuda_raytracer.cuh:43-55).
 enum Legacy : int {
@@ -445,6 +461,24 @@ struct HitInfo {
   int sdf_mat;
 };
 
+// Both child boxes of quantised node `cur` tested against the ray (two
+// 128-bit loads from one 32-byte sector); f3v = (left, right, split axis).
+// Each bound decodes as corner + q * step in one rounding (q * step is exact).
+__device__ __forceinline__ void qnode_visit(const SceneView &S, const RayPre &rp, int cur, float tmin, float closest,
+                                            bool &hl, float &tl, bool &hr, float &tr, int4 &f3v) {
+  const uint4 *n = reinterpret_cast<const uint4 *>(S.qnodes + cur);
+  const uint4 a = __ldg(n), b = __ldg(n + 1);  // (ox, oy, oz, lq0), (lq1, rq, left, right)
+  const float ox = qnode_origin(a.x), oy = qnode_origin(a.y), oz = qnode_origin(a.z);
+  const float sx = qnode_step(a.x), sy = qnode_step(a.y), sz = qnode_step(a.z);
+#define RB_DQ(word, sh, o, s) fmaf((float)(((word) >> (sh)) & 0xFFu), (s), (o))
+  hl = box_hit(rp, RB_DQ(a.w, 0, ox, sx), RB_DQ(a.w, 8, oy, sy), RB_DQ(a.w, 16, oz, sz), RB_DQ(a.w, 24, ox, sx),
+               RB_DQ(b.x, 0, oy, sy), RB_DQ(b.x, 8, oz, sz), tmin, closest, tl);
+  hr = box_hit(rp, RB_DQ(b.x, 16, ox, sx), RB_DQ(b.x, 24, oy, sy), RB_DQ(b.y, 0, oz, sz), RB_DQ(b.y, 8, ox, sx),
+               RB_DQ(b.y, 16, oy, sy), RB_DQ(b.y, 24, oz, sz), tmin, closest, tr);
+#undef RB_DQ
+  f3v = make_int4((int)b.z, (int)b.w, (int)((a.x & 1u) | ((a.y & 1u) << 1)), 0);
+}
+
 static __device__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax, SdfCand &c,
                                        float &t, f3 &n, int &mat);
 
@@ -562,20 +596,7 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
         hl = box_hit(rp, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, tmin, closest, tl);
         hr = box_hit(rp, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, tmin, closest, tr);
       } else {
-        const float4 *n = reinterpret_cast<const float4 *>(S.qnodes + cur);
-        const float4 q0 = __ldg(n);
-        const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(n + 1));
-        const int rref = __ldg(reinterpret_cast<const int *>(n + 2));
-        const uint32_t meta = __float_as_uint(q0.w);
-        const float sx = __uint_as_float((meta & 0xFFu) << 23), sy = __uint_as_float(((meta >> 8) & 0xFFu) << 23),
-                    sz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
-#define RB_DQ(word, sh, o, s) fmaf((float)(((word) >> (sh)) & 0xFFu), (s), (o))
-        hl = box_hit(rp, RB_DQ(q1.x, 0, q0.x, sx), RB_DQ(q1.x, 8, q0.y, sy), RB_DQ(q1.x, 16, q0.z, sz),
-                     RB_DQ(q1.x, 24, q0.x, sx), RB_DQ(q1.y, 0, q0.y, sy), RB_DQ(q1.y, 8, q0.z, sz), tmin, closest, tl);
-        hr = box_hit(rp, RB_DQ(q1.y, 16, q0.x, sx), RB_DQ(q1.y, 24, q0.y, sy), RB_DQ(q1.z, 0, q0.z, sz),
-                     RB_DQ(q1.z, 8, q0.x, sx), RB_DQ(q1.z, 16, q0.y, sy), RB_DQ(q1.z, 24, q0.z, sz), tmin, closest, tr);
-#undef RB_DQ
-        f3v = make_int4((int)q1.w, rref, (int)(meta >> 24), 0);
+        qnode_visit(S, rp, cur, tmin, closest, hl, tl, hr, tr, f3v);
       }
       const float dcomp = f3v.z == 0 ? ray.d.x : (f3v.z == 1 ? ray.d.y : ray.d.z);
       const bool left_near = dcomp >= 0.0f;
@@ -634,20 +655,7 @@ __device__ __forceinline__ void visit_interior(const SceneView &S, const RayPre 
     hl = box_hit(rp, f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, tmin, closest, tl);
     hr = box_hit(rp, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, tmin, closest, tr);
   } else {
-    const float4 *n = reinterpret_cast<const float4 *>(S.qnodes + cur);
-    const float4 q0 = __ldg(n);
-    const uint4 q1 = __ldg(reinterpret_cast<const uint4 *>(n + 1));
-    const int rref = __ldg(reinterpret_cast<const int *>(n + 2));
-    const uint32_t meta = __float_as_uint(q0.w);
-    const float sx = __uint_as_float((meta & 0xFFu) << 23), sy = __uint_as_float(((meta >> 8) & 0xFFu) << 23),
-                sz = __uint_as_float(((meta >> 16) & 0xFFu) << 23);
-#define RB_DQ(word, sh, o, s) fmaf((float)(((word) >> (sh)) & 0xFFu), (s), (o))
-    hl = box_hit(rp, RB_DQ(q1.x, 0, q0.x, sx), RB_DQ(q1.x, 8, q0.y, sy), RB_DQ(q1.x, 16, q0.z, sz),
-                 RB_DQ(q1.x, 24, q0.x, sx), RB_DQ(q1.y, 0, q0.y, sy), RB_DQ(q1.y, 8, q0.z, sz), tmin, closest, tl);
-    hr = box_hit(rp, RB_DQ(q1.y, 16, q0.x, sx), RB_DQ(q1.y, 24, q0.y, sy), RB_DQ(q1.z, 0, q0.z, sz),
-                 RB_DQ(q1.z, 8, q0.x, sx), RB_DQ(q1.z, 16, q0.y, sy), RB_DQ(q1.z, 24, q0.z, sz), tmin, closest, tr);
-#undef RB_DQ
-    f3v = make_int4((int)q1.w, rref, (int)(meta >> 24), 0);
+    qnode_visit(S, rp, cur, tmin, closest, hl, tl, hr, tr, f3v);
   }
   const float dcomp = f3v.z == 0 ? ray.d.x : (f3v.z == 1 ? ray.d.y : ray.d.z);
   const bool left_near = dcomp >= 0.0f;

@@ -13,6 +13,20 @@ def _orbit_frames(spec, n, w, h):
     return [scenes.orbit(spec.camera, 2 * np.pi * v / n).frame(w, h) for v in range(n)]
 
 
+def _paired(a, b, spp, name):
+    """Same sample streams. Triangle scenes agree pixel for pixel; on the
+    smooth SDF field the two kernels (compiled separately) may round a march
+    step differently in the last bit, and a path that then branches
+    differently changes its pixel, so a few pixels may differ (the paired
+    tolerance of the other SDF engine comparisons) while the images agree."""
+    if name != "sdf_field":
+        np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-4 * spp)
+        return
+    bad = (np.abs(a - b) > 1e-4 * (1 + np.abs(b)) * spp).any(axis=-1)
+    assert bad.mean() < 0.01, bad.mean()
+    np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=1e-2)
+
+
 @pytest.mark.parametrize("name", ["cornell", "sdf_field"])
 def test_views_match_single_frames(cuda, name):
     spec = scenes.sdf_field(count=48) if name == "sdf_field" else scenes.cornell()
@@ -26,14 +40,14 @@ def test_views_match_single_frames(cuda, name):
     assert cnt[1] == n * w * h * spp and cnt[0] >= cnt[1]
     # view 0 draws salt 0, the streams of rb_render_accumulate
     ref0 = render.render_accumulate(ds, frames[0], w, h, spp, spec.depth, background=spec.background)
-    np.testing.assert_allclose(imgs[0], ref0, rtol=1e-4, atol=1e-4 * spp)
+    _paired(imgs[0], ref0, spp, name)
     # view v draws salt v: the server's job with seed (salt) v
     srv = serving.Server(paths_per_iteration=1 << 24, max_spp_per_iteration=spp)
     sid = srv.add_scene(ds)
     for v in range(1, n):
         j = srv.submit(serving.job(sid, frames[v], w, h, spp, spec.depth, background=spec.background, seed=v))
         srv.drain()
-        np.testing.assert_allclose(imgs[v], srv.fetch(j, w, h), rtol=1e-4, atol=1e-4 * spp)
+        _paired(imgs[v], srv.fetch(j, w, h), spp, name)
     srv.close()
     ds.free()
 
