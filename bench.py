@@ -665,7 +665,7 @@ def main():
         res["rmse_vs_oracle"] = config_error(args.workload, step, acc, engine, nviews, npx, spp, w, h)
     if args.workload == "icospheres" and not args.small:
         # the configuration asks for 8-bit quantised child bounds vs FP32 nodes
-        res["quantized_bvh"] = quantized_compare(sc, fr, w, h, spp, depth, step_ms=t_ms)
+        res["node_layouts"] = node_layout_compare(sc, fr, w, h, spp, depth, step_ms=t_ms)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             res["cpu_baseline"] = cpu_baseline(args.workload)
@@ -720,18 +720,21 @@ def sample_split_section(ds, fr, w, h, spp, depth, spec, engine, world):
     return out
 
 
-def quantized_compare(sc, fr, w, h, spp, depth, step_ms):
-    """One frame on the 8-bit quantised BVH (48 B nodes) of the same tree against
-    the FP32-node tree, both uploaded as built with the class's default launch
-    configuration (the same kernel, the same samples), median of 3 frames each."""
+def node_layout_compare(sc, fr, w, h, spp, depth, step_ms):
+    """One frame on each node layout of the same tree, uploaded as built with
+    the class's default launch configuration (the same kernel, the same
+    samples), median of 3 frames each: the binary tree with FP32 boxes (64 B
+    nodes), the binary tree with 8-bit quantised boxes (32 B nodes) and the
+    4-wide copy with FP32 boxes (128 B nodes, the default)."""
     import torch
 
     from rayon_b200 import lib
     out = {}
     frp = np.ascontiguousarray(fr, np.float64).ctypes.data_as(C.POINTER(C.c_double))
     acc = torch.zeros((w * h * 2, 4), dtype=torch.float32, device="cuda")
-    for name, q in (("fp32", False), ("quantized", True)):
-        d = sc.upload(quantized=q)
+    for name, kw in (("binary_fp32", dict(wide=False)), ("binary_quantized", dict(quantized=True)),
+                     ("wide_fp32", dict(wide=True))):
+        d = sc.upload(**kw)
         args = (d.handle, w, h, frp, spp, 0, depth, C.c_void_p(acc.data_ptr()),
                 C.c_void_p(acc.data_ptr() + w * h * 16), None, None)
         lib.rb_render_accumulate(*args)
@@ -747,7 +750,8 @@ def quantized_compare(sc, fr, w, h, spp, depth, step_ms):
         m = statistics.median(ms)
         out[name] = {"ms_per_frame": m, "mpaths_s": w * h * spp / (m * 1e-3) / 1e6, "device_bytes": d.nbytes}
         d.free()
-    out["quantized_over_fp32_time"] = out["quantized"]["ms_per_frame"] / out["fp32"]["ms_per_frame"]
+    out["quantized_over_binary_time"] = out["binary_quantized"]["ms_per_frame"] / out["binary_fp32"]["ms_per_frame"]
+    out["wide_over_binary_time"] = out["wide_fp32"]["ms_per_frame"] / out["binary_fp32"]["ms_per_frame"]
     out["tuned_timed_step_ms"] = step_ms
     return out
 

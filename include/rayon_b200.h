@@ -231,6 +231,10 @@ typedef struct rb_upload_opts {
   const double *probe_frame;      /* autotune on this camera (rb_camera_frame), or NULL */
   int traversal_budget;           /* testing: traversal step budget per ray (0: 2 * (primitives + 4) + 64,
                                      which no well-formed tree reaches) */
+  int wide_bvh;                   /* 0 (default) or 1: the render kernels traverse a 4-wide copy of
+                                     the BVH (the same FP32 child boxes and leaves, four per 128-byte
+                                     node); primary hits and exact-order traversal keep the binary
+                                     tree. -1: binary tree only. Not with quantized_bvh. */
 } rb_upload_opts;
 
 /* RB_LAYOUT_AS_BUILT: the scene's BVH as built (the reference's leaf-4 tree
@@ -301,7 +305,12 @@ typedef struct rb_render_opts {
                            [1]: sample slices per pixel of the per-pixel kernel
                            (0 = automatic: frames with fewer pixels than four
                            times the GPU's resident threads split their samples,
-                           up to 8 slices) */
+                           up to 8 slices);
+                           [2]: schedule of the per-pixel kernel: 1 grid (one
+                           thread per pixel of a 2-D grid), 2 fetch (a persistent
+                           grid whose warps take 8x4-pixel tiles of a sample
+                           slice from a counter; the same sums bit for bit);
+                           0 = the scene's tuned schedule, fetch by default) */
 } rb_render_opts;
 void rb_get_render_opts(rb_render_opts *out);
 void rb_set_render_opts(const rb_render_opts *in);

@@ -59,7 +59,7 @@ class MaterialDesc(C.Structure):
 class UploadOpts(C.Structure):
     _fields_ = [("quantized_bvh", C.c_int), ("use_bvh", C.c_int), ("layout", C.c_int), ("max_leaf", C.c_int),
                 ("tune_depth", C.c_int), ("probe_width", C.c_int), ("probe_height", C.c_int),
-                ("probe_frame", C.POINTER(C.c_double)), ("traversal_budget", C.c_int)]
+                ("probe_frame", C.POINTER(C.c_double)), ("traversal_budget", C.c_int), ("wide_bvh", C.c_int)]
 
 
 LAYOUT_AS_BUILT, LAYOUT_AUTOTUNE, LAYOUT_LINEAR, LAYOUT_LEAF = 0, 1, 2, 3

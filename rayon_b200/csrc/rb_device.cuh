@@ -166,6 +166,7 @@ static_assert(sizeof(SdfPrim) == 80, "SdfPrim is five 16-byte words");
 struct SceneView {
   const float4 *__restrict__ nodes;
   const QNode *__restrict__ qnodes;
+  const float4 *__restrict__ wnodes;  // 4-wide copy of the tree (render kernels) or null
   const float4 *__restrict__ prims;
   const float4 *__restrict__ normals;  // 3 x float4 per primitive or null
   const DevMaterial *__restrict__ mats;
@@ -187,6 +188,7 @@ struct SceneView {
   float sdf_eps;
   int trav_budget;     // traversal step budget override (0: 2 * (prims + 4) + 64)
   int short_stack;     // traversal stack entries in shared memory (0: RB_SHORT)
+  int wide_root;       // root of wnodes
   // Rays whose traversal ran out of its step budget (a corrupt tree; never a
   // well-formed one): counted here, read by rb_scene_traversal_faults.
   unsigned long long *faults;
@@ -351,16 +353,14 @@ struct SdfMask {
   }
 };
 
+// The closest-hit test of primitive i given its record's three words.
 template <int MS, class Sink = SdfCand>
-__device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
-                                       float &t, Sink *cand = nullptr) {
-  const float4 *p = S.prims + 3 * (size_t)i;
-  const float4 a = __ldg(p);
-  const float4 c = __ldg(p + 2);
+__device__ __forceinline__ bool prim_t_words(const SceneView &S, int i, const float4 &a, const float4 &b,
+                                             const float4 &c, const Ray &r, float tmin, float tmax, float &t,
+                                             Sink *cand = nullptr) {
   const uint32_t tag = __float_as_uint(c.w);
   const uint32_t kind = tag_kind(tag);
   if (kind == PK_SPHERE || kind == PK_DISPLACED) return t_sphere(f3(a.x, a.y, a.z), a.w, r, tmin, tmax, t);
-  const float4 b = __ldg(p + 1);
   if (kind == PK_TRI)
     return t_tri(f3(a.x, a.y, a.z), f3(a.w, b.x, b.y), f3(b.z, b.w, c.x), r, tmin, tmax, t);
   if (kind == PK_RECT)
@@ -383,6 +383,19 @@ __device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, 
   }
   return false;
 }
+
+// The test with the record loaded here: all three words in one round trip
+// (the kind tag is in the last word; loading the middle word only after
+// testing it would put a second dependent memory latency on every triangle
+// and quad test).
+template <int MS, class Sink = SdfCand>
+__device__ __forceinline__ bool prim_t(const SceneView &S, int i, const Ray &r, float tmin, float tmax,
+                                       float &t, Sink *cand = nullptr) {
+  const float4 *p = S.prims + 3 * (size_t)i;
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  return prim_t_words<MS, Sink>(S, i, a, b, c, r, tmin, tmax, t, cand);
+}
+
 
 // ---------------------------------------------------------------------------
 // Traversal (hit_scene, cuda_raytracer.cuh:487-602)
@@ -640,7 +653,9 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
 // full warps instead of alternating per iteration. Leaves are tested in the
 // same front-to-back order; postponing only makes culling by the closest hit
 // less eager, so a hit can differ from the exact-order traversal only where a
-// primitive test and its box test disagree by a rounding step.
+// primitive test and its box test disagree by a rounding step. A scene
+// uploaded with a 4-wide copy of its tree (SceneView::wnodes) is traversed on
+// that copy: the same child boxes and leaves, four per visit (visit_wide).
 #define RB_TRAV_DONE 0x7FFFFFFF
 
 __device__ __forceinline__ void visit_interior(const SceneView &S, const RayPre &rp, const Ray &ray, int cur, float tmin,
@@ -675,6 +690,41 @@ __device__ __forceinline__ void visit_interior(const SceneView &S, const RayPre 
   }
 }
 
+// One 4-wide node (wide_bvh.cu: 128 B, bounds of the four children in the
+// lanes of six words, then the child refs): the hit children are ordered by
+// entry distance with a five-exchange sorting network, the farther ones pushed
+// from far to near so that the nearest pending child is popped first, and the
+// nearest becomes `next`.
+__device__ __forceinline__ void visit_wide(const SceneView &S, const RayPre &rp, int cur, float tmin, float closest,
+                                           int &next, Stack &st, uint32_t &overflow) {
+  const float4 *n = S.wnodes + 8 * (size_t)cur;
+  const float4 lx = __ldg(n), hx = __ldg(n + 1), ly = __ldg(n + 2), hy = __ldg(n + 3), lz = __ldg(n + 4),
+               hz = __ldg(n + 5);
+  const int4 rf = __ldg(reinterpret_cast<const int4 *>(n + 6));
+  const float INF = __int_as_float(0x7f800000);
+  float k0, k1, k2, k3;
+  int r0 = rf.x, r1 = rf.y, r2 = rf.z, r3 = rf.w;
+  k0 = box_hit(rp, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, tmin, closest, k0) ? k0 : INF;
+  k1 = box_hit(rp, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, tmin, closest, k1) ? k1 : INF;
+  k2 = box_hit(rp, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, tmin, closest, k2) ? k2 : INF;
+  k3 = box_hit(rp, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, tmin, closest, k3) ? k3 : INF;
+#define RB_CX(a, b)                                       \
+  if (k##b < k##a) {                                      \
+    const float tk = k##a; k##a = k##b; k##b = tk;        \
+    const int tr = r##a; r##a = r##b; r##b = tr;          \
+  }
+  RB_CX(0, 1) RB_CX(2, 3) RB_CX(0, 2) RB_CX(1, 3) RB_CX(1, 2)
+#undef RB_CX
+#define RB_PUSH_W(k, r)                     \
+  if (k < INF) {                            \
+    if (st.sp < RB_STACK) st.push(r, k);    \
+    else ++overflow;                        \
+  }
+  RB_PUSH_W(k3, r3) RB_PUSH_W(k2, r2) RB_PUSH_W(k1, r1)
+#undef RB_PUSH_W
+  next = k0 < INF ? r0 : RB_TRAV_DONE;
+}
+
 __device__ __forceinline__ int pop_next(Stack &st, float closest) {
   while (st.sp > 0) {
     const int2 e = st.pop();
@@ -696,7 +746,8 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
                closest, te))
     return h;
   st.sp = 0;
-  int node = S.root_ref;
+  const bool wide = S.wnodes != nullptr;
+  int node = wide ? S.wide_root : S.root_ref;
   int leaf = RB_TRAV_DONE;  // postponed leaf
   // every interior node and every leaf is visited at most once, so this
   // budget is never reached by a well-formed tree; it bounds a corrupt one
@@ -705,7 +756,8 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
     // interior phase
     while (node != RB_TRAV_DONE && !ref_is_leaf(node) && --budget > 0) {
       int next;
-      visit_interior(S, rp, ray, node, tmin, closest, next, st, overflow);
+      if (wide) visit_wide(S, rp, node, tmin, closest, next, st, overflow);
+      else visit_interior(S, rp, ray, node, tmin, closest, next, st, overflow);
       node = next == RB_TRAV_DONE ? pop_next(st, closest) : next;
       if (node != RB_TRAV_DONE && ref_is_leaf(node) && leaf == RB_TRAV_DONE) {
         leaf = node;  // postpone and keep descending

@@ -54,6 +54,7 @@ struct uninit_alloc : std::allocator<T> {
 struct HostLayout {
   std::vector<float4, uninit_alloc<float4>> nodes;  // 4 per interior node, every word written
   std::vector<rbd::QNode> qnodes;     // quantised copy of nodes
+  std::vector<float4> wnodes;         // 4-wide copy of nodes (8 per wide node) or empty
   std::vector<float4, uninit_alloc<float4>> prims;  // 3 per primitive, zeroed record by record
   std::vector<float4> normals;        // 3 per primitive (vertex normals) or empty
   std::vector<rbd::DevMaterial> mats;
@@ -61,6 +62,7 @@ struct HostLayout {
   std::vector<rbd::SdfPrim> sdf;
   std::vector<float4> groups;         // grouped linear layout: 2 per group
   int root_ref = 0;
+  int wide_root = 0;                  // root of wnodes (a leaf ref when the root is a leaf)
   float root_box[6] = {0, 0, 0, 0, 0, 0};
   float light_area = 0.0f;
   bool use_bvh = false;
@@ -76,6 +78,7 @@ struct DeviceScene {
   float probe_ms = 0.0f;
   // launch configuration chosen by the autotuner (0: the class defaults)
   int tuned_minb = 0, tuned_bx = 0, tuned_by = 0;
+  int tuned_fetch = 0;  // k_render schedule: 0 default (fetch), 1 grid, 2 fetch
   int wf_queue = 0;          // wavefront engine path slots for this scene (0: default)
   bool tune_cached = false;  // the decision came from the per-(GPU, scene) cache
 };
@@ -119,6 +122,8 @@ enum AllocSite { RB_SITE_SERVER_JOB = 0, RB_SITE_WAVEFRONT = 1, RB_SITE_COUNT = 
 bool injected_alloc_failure(int site);
 DeviceScene *lookup_scene(const void *handle);
 void build_quantized(HostLayout &L);
+// Fills L.wnodes / L.wide_root from the binary nodes (wide_bvh.cu).
+void build_wide(HostLayout &L);
 FrameF frame_from(const double *fr, int w, int h);
 // The per-frame kernel over one frame's sample range (rb_render.cu).
 int launch_render(const DeviceScene *ds, const rbd::Globals &G, const FrameF &P, float4 *acc, float4 *comp,

@@ -7,8 +7,10 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -331,6 +333,7 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     const Node &root = hs.nodes[hs.root];
     for (int k = 0; k < 3; ++k) { L.root_box[k] = (float)root.bmin[k]; L.root_box[3 + k] = (float)root.bmax[k]; }
     L.root_ref = ref_of(hs.root);
+    if (opts.wide_bvh >= 0 && !opts.quantized_bvh) build_wide(L);  // 0: default on
     if (opts.quantized_bvh) {
       build_quantized(L);
       L.nodes.clear();  // the quantised copy replaces the FP32 nodes on the device
@@ -377,6 +380,7 @@ static bool build_device_layout(const HostScene &hs, const rb_upload_opts &opts,
     L.use_bvh = false;
     L.nodes.clear();
     L.qnodes.clear();
+    L.wnodes.clear();
   }
   return true;
 }
@@ -395,6 +399,7 @@ void free_device_scene(DeviceScene *ds) {
   if (!ds) return;
   cudaFree((void *)ds->view.nodes);
   cudaFree((void *)ds->view.qnodes);
+  cudaFree((void *)ds->view.wnodes);
   cudaFree((void *)ds->view.prims);
   cudaFree((void *)ds->view.normals);
   cudaFree((void *)ds->view.mats);
@@ -418,14 +423,17 @@ DeviceScene *upload_scene(const HostScene &hs, const rb_upload_opts &opts, cudaS
   LightRec *lights = nullptr;
   SdfPrim *sdf = nullptr;
   float4 *groups = nullptr;
+  float4 *wn = nullptr;
   bool ok = upload_vec(L.nodes, &nodes, st, bytes) && upload_vec(L.qnodes, &qn, st, bytes) &&
+            upload_vec(L.wnodes, &wn, st, bytes) &&
             upload_vec(L.prims, &prims, st, bytes) && upload_vec(L.normals, &normals, st, bytes) &&
             upload_vec(L.mats, &mats, st, bytes) && upload_vec(L.lights, &lights, st, bytes) &&
             upload_vec(L.sdf, &sdf, st, bytes) && upload_vec(L.groups, &groups, st, bytes);
-  v.nodes = nodes; v.qnodes = qn; v.prims = prims; v.normals = normals; v.mats = mats;
+  v.nodes = nodes; v.qnodes = qn; v.wnodes = wn; v.prims = prims; v.normals = normals; v.mats = mats;
   v.lights = lights; v.sdf = sdf; v.groups = groups;
   v.num_groups = (int)(L.groups.size() / 2);
   v.root_ref = L.root_ref;
+  v.wide_root = L.wide_root;
   v.num_prims = (int)hs.geoms.size();
   v.num_mats = (int)hs.materials.size();
   v.num_lights = (int)L.lights.size();
@@ -494,20 +502,16 @@ __global__ void __launch_bounds__(256) k_primary(const RB_GRID_CONST SceneView S
   if (tout) tout[pix] = h.prim >= 0 ? h.t : -1.0f;
 }
 
-// Per-pixel progressive kernel: one thread owns one pixel for the launch and
-// runs its samples back to back in a single flattened loop (one path segment
-// per iteration), so a lane whose path ended starts its next sample at once
-// instead of idling until the warp's longest path finishes.
-template <bool NEE, int MS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneView S,
-                                                      const RB_GRID_CONST Globals G,
-                                                      const RB_GRID_CONST FrameF P, float4 *__restrict__ acc,
-                                                float4 *__restrict__ comp, float4 *__restrict__ part,
-                                                int *__restrict__ counts, unsigned long long *__restrict__ counters) {
-  extern __shared__ int2 smem[];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+// One pixel's sample slice z of nz: the pixel's samples of the slice back to
+// back in one flattened loop (one path segment per iteration). Adds the
+// thread's segments and paths to segs and paths.
+template <bool NEE, int MS>
+__device__ __forceinline__ void render_pixel_slice(const SceneView &S, const Globals &G, const FrameF &P, int x, int y,
+                                                   int z, int nz, int2 *smem, int tid, int threads,
+                                                   float4 *__restrict__ acc, float4 *__restrict__ comp,
+                                                   float4 *__restrict__ part, int *__restrict__ counts,
+                                                   unsigned long long *__restrict__ counters,
+                                                   unsigned long long &segs, unsigned long long &paths) {
   const bool inside = x < P.width && y < P.height;
   const int pix = inside ? y * P.width + x : 0;
   int have = 0;
@@ -516,17 +520,15 @@ __global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneV
     have = counts[pix];
     if (have < 0) work = false;  // converged (sign bit, render_acc_kernel.cu:165-170)
   }
-  unsigned long long segs = 0;
   if (work) {
     Stack st;
-    stack_init(st, smem, tid, blockDim.x * blockDim.y, S.short_stack);
+    stack_init(st, smem, tid, threads, S.short_stack);
     uint32_t ovf = 0;
-    // sample slice blockIdx.z of gridDim.z (small frames split their samples
-    // so that the launch fills the GPU): slice 0 adds into the pixel's sums,
-    // the others leave partial sums in part for k_fold_slices
-    const int z = blockIdx.z;
-    const int s_begin = (int)((long long)P.samples * z / gridDim.z);
-    const int s_end = (int)((long long)P.samples * (z + 1) / gridDim.z);
+    // sample slice z of nz (small frames split their samples so that the
+    // launch fills the GPU): slice 0 adds into the pixel's sums, the others
+    // leave partial sums in part for k_fold_slices
+    const int s_begin = (int)((long long)P.samples * z / nz);
+    const int s_end = (int)((long long)P.samples * (z + 1) / nz);
     float sx = 0.f, sy = 0.f, sz = 0.f;
     float cx = 0.f, cy = 0.f, cz = 0.f;
     if (z == 0) {
@@ -591,18 +593,72 @@ __global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneV
       }
     }
     if (counters && ovf) atomicAdd(counters + 2, (unsigned long long)ovf);
+    paths += (unsigned long long)(s_end - s_begin);
+  }
+}
+
+// Per-pixel progressive kernel: one thread owns one pixel for the launch and
+// runs its samples back to back in a single flattened loop (one path segment
+// per iteration), so a lane whose path ended starts its next sample at once
+// instead of idling until the warp's longest path finishes.
+//
+// Two schedules of the same work. Grid mode (fetch == nullptr): one thread per
+// pixel of a 2-D grid of bx x by blocks, sample slice blockIdx.z of gridDim.z.
+// Fetch mode: a persistent grid of 1-D blocks sized to the SMs' resident
+// capacity; each warp takes work items (a tile of 8 x 4 pixels in one sample
+// slice of `nslices`) from the counter *fetch until they run out, so a warp
+// whose tile finished early starts the next one instead of idling until its
+// block's other warps and the launch's last wave finish. Items run slice-major,
+// then tile rows, so concurrent warps work on neighbouring tiles. A pixel's
+// slice is computed by one thread in sample order either way: the sums are the
+// same bit for bit.
+#define RB_TILE_W 8
+#define RB_TILE_H 4
+template <bool NEE, int MS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneView S,
+                                                      const RB_GRID_CONST Globals G,
+                                                      const RB_GRID_CONST FrameF P, float4 *__restrict__ acc,
+                                                float4 *__restrict__ comp, float4 *__restrict__ part,
+                                                int *__restrict__ counts, unsigned long long *__restrict__ counters,
+                                                int *__restrict__ fetch, int nslices) {
+  extern __shared__ int2 smem[];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int threads = blockDim.x * blockDim.y;
+  const int lane = tid & 31;
+  const int tiles_x = (P.width + RB_TILE_W - 1) / RB_TILE_W;
+  const int tiles = tiles_x * ((P.height + RB_TILE_H - 1) / RB_TILE_H);
+  const long long items = fetch ? (long long)tiles * nslices : 0;
+  unsigned long long segs = 0, paths = 0;
+  for (;;) {
+    int x, y, z, nz;
+    if (fetch) {
+      int it = 0;
+      if (lane == 0) it = atomicAdd(fetch, 1);
+      it = __shfl_sync(0xffffffffu, it, 0);
+      if (it >= items) break;
+      z = it / tiles;
+      const int tile = it - z * tiles;
+      const int ty = tile / tiles_x;
+      x = (tile - ty * tiles_x) * RB_TILE_W + (lane & (RB_TILE_W - 1));
+      y = ty * RB_TILE_H + lane / RB_TILE_W;
+      nz = nslices;
+    } else {
+      x = blockIdx.x * blockDim.x + threadIdx.x;
+      y = blockIdx.y * blockDim.y + threadIdx.y;
+      z = blockIdx.z;
+      nz = gridDim.z;
+    }
+    render_pixel_slice<NEE, MS>(S, G, P, x, y, z, nz, smem, tid, threads, acc, comp, part, counts, counters, segs,
+                                paths);
+    if (!fetch) break;
   }
   if (counters) {
     // warp-aggregated segment and path counts
-    unsigned long long paths =
-        work ? (unsigned long long)((long long)P.samples * (blockIdx.z + 1) / gridDim.z -
-                                    (long long)P.samples * blockIdx.z / gridDim.z)
-             : 0ull;
     for (int o = 16; o > 0; o >>= 1) {
       segs += __shfl_down_sync(0xffffffffu, segs, o);
       paths += __shfl_down_sync(0xffffffffu, paths, o);
     }
-    if ((tid & 31) == 0) {
+    if (lane == 0) {
       atomicAdd(counters, segs);
       atomicAdd(counters + 1, paths);
     }
@@ -758,13 +814,28 @@ static void default_block(int ms, int &bx, int &by) {
 template <bool NEE, int MS>
 static void launch_ms(int minb, dim3 grd, dim3 blk, size_t sm, cudaStream_t st, const SceneView &S, const Globals &G,
                       const FrameF &P, float4 *acc, float4 *comp, float4 *part, int *counts,
-                      unsigned long long *counters) {
+                      unsigned long long *counters, int *fetch, int nslices) {
   switch (minb) {
-    case 1: k_render<NEE, MS, 1><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters); break;
-    case 3: k_render<NEE, MS, 3><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters); break;
-    case 4: k_render<NEE, MS, 4><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters); break;
-    default: k_render<NEE, MS, 2><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters); break;
+    case 1: k_render<NEE, MS, 1><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
+    case 3: k_render<NEE, MS, 3><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
+    case 4: k_render<NEE, MS, 4><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
+    default: k_render<NEE, MS, 2><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
   }
+}
+
+// Resident blocks per SM of k_render<NEE, MS, minb> at `threads` threads and
+// `sm` bytes of dynamic shared memory (the persistent grid of fetch mode).
+template <bool NEE, int MS>
+static int resident_blocks(int minb, int threads, size_t sm) {
+  int n = 0;
+  cudaError_t e;
+  switch (minb) {
+    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 1>, threads, sm); break;
+    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 3>, threads, sm); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 4>, threads, sm); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 2>, threads, sm); break;
+  }
+  return e == cudaSuccess && n > 0 ? n : 1;
 }
 
 // Stream-ordered scratch of the sample slices: a private memory pool per
@@ -816,6 +887,39 @@ static cudaEvent_t ktimer_mark(cudaStream_t st) {
   return e;
 }
 
+// Fetch mode's block size (two warps) and its resident blocks per SM per
+// kernel instance (cached: the occupancy query is a driver call).
+#define RB_FETCH_THREADS 64
+static int fetch_resident_blocks(int ms, bool nee, int minb, int sm) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, int>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, ms * 2 + (nee ? 1 : 0), minb, sm, (int)RB_FETCH_THREADS);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int n = 1;
+#define RB_RES(NEE_, MS_) n = resident_blocks<NEE_, MS_>(minb, RB_FETCH_THREADS, (size_t)sm)
+  if (nee) {
+    if (ms == RB_MS_DIFFUSE) RB_RES(true, RB_MS_DIFFUSE);
+    else if (ms == RB_MS_CLASSIC) RB_RES(true, RB_MS_CLASSIC);
+    else if (ms == RB_MS_FULL) RB_RES(true, RB_MS_FULL);
+    else RB_RES(true, RB_MS_SDF);
+  } else {
+    if (ms == RB_MS_DIFFUSE) RB_RES(false, RB_MS_DIFFUSE);
+    else if (ms == RB_MS_CLASSIC) RB_RES(false, RB_MS_CLASSIC);
+    else if (ms == RB_MS_FULL) RB_RES(false, RB_MS_FULL);
+    else RB_RES(false, RB_MS_SDF);
+  }
+#undef RB_RES
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = n;
+  return n;
+}
+
 int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, int *counts,
                   unsigned long long *counters, cudaStream_t st) {
   const rb_render_opts o = current_opts();
@@ -826,9 +930,19 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
     bx = ds->tuned_bx;
     by = ds->tuned_by;
   }
-  if (o.block_x > 0 && o.block_y > 0 && o.block_x * o.block_y <= 256 && o.block_x * o.block_y >= 32) {
+  // (whole warps: the kernel's warp shuffles take every lane)
+  if (o.block_x > 0 && o.block_y > 0 && o.block_x * o.block_y <= 256 && o.block_x * o.block_y % 32 == 0) {
     bx = o.block_x;
     by = o.block_y;
+  }
+  // schedule: rb_render_opts.reserved[2] (1 grid, 2 fetch), else the scene's
+  // tuned one, else fetch (measured on B200 against the grid at the same
+  // register budget: icospheres 1920x1080 x 64 spp 33.6 -> 31.9 ms,
+  // One-Weekend 400x225 x 32 spp 0.906 -> 0.869 ms, Cornell equal)
+  const bool fetch_mode = o.reserved[2] > 0 ? o.reserved[2] == 2 : ds->tuned_fetch != 1;
+  if (fetch_mode) {
+    bx = RB_FETCH_THREADS;
+    by = 1;
   }
   dim3 blk(bx, by), grd((P.width + bx - 1) / bx, (P.height + by - 1) / by);
   const size_t sm = stack_smem_bytes(ds->view.short_stack, blk.x * blk.y);
@@ -837,6 +951,9 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   // the class default
   const int minb = o.reserved[0] > 0 ? o.reserved[0]
                    : (ds->tuned_minb > 0 && !G.nee) ? ds->tuned_minb : default_minb(ms, G.nee != 0);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // A frame with fewer pixels than four times the GPU's resident threads
   // splits its samples into up to 8 slices (grid z), so that the launch keeps
   // the GPU full to its end (measured on B200: 400x225 x 32 spp 1.99 -> 1.13 ms,
@@ -850,22 +967,39 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
     if (o.reserved[1] > 0) {  // explicit slice count (rb_render_opts.reserved[1])
       slices = std::min(std::min(o.reserved[1], 64), P.samples);
     } else {
-      int dev = 0, sms = 148;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       const long long resident = (long long)sms * minb * 256;
       while (slices < 8 && slices * 2 <= P.samples && npix * slices < 4 * resident) slices *= 2;
     }
   }
-  float4 *part = nullptr;
-  cudaMemPool_t pool = slices > 1 ? scratch_pool() : nullptr;
-  if (slices > 1 && (!pool || !cuda_ok(cudaMallocFromPoolAsync((void **)&part,
-                                                               sizeof(float4) * (size_t)npix * (slices - 1), pool, st),
-                                       "slice scratch")))
-    slices = 1;
-  grd.z = slices;
+  // one scratch allocation: the slices' partial sums, then fetch mode's work
+  // counter (16-byte aligned after them)
+  const size_t part_bytes = sizeof(float4) * (size_t)npix * (slices - 1);
+  const size_t scratch_bytes = part_bytes + (fetch_mode ? 16 : 0);
+  char *scratch = nullptr;
+  if (scratch_bytes > 0) {
+    cudaMemPool_t pool = scratch_pool();
+    if (!pool || !cuda_ok(cudaMallocFromPoolAsync((void **)&scratch, scratch_bytes, pool, st), "launch scratch")) {
+      if (fetch_mode) return RB_ERR_OUT_OF_MEMORY;
+      slices = 1;  // the grid schedule renders without scratch
+      scratch = nullptr;
+    }
+  }
+  float4 *part = slices > 1 ? reinterpret_cast<float4 *>(scratch) : nullptr;
+  int *fetch = nullptr;
+  if (fetch_mode) {
+    fetch = reinterpret_cast<int *>(scratch + part_bytes);
+    cudaMemsetAsync(fetch, 0, sizeof(int), st);
+    const long long items = (long long)((P.width + RB_TILE_W - 1) / RB_TILE_W) *
+                            ((P.height + RB_TILE_H - 1) / RB_TILE_H) * slices;
+    const long long per_sm = fetch_resident_blocks(ds->ms, G.nee != 0, minb, (int)sm);
+    const long long warps_per_block = RB_FETCH_THREADS / 32;
+    grd = dim3((unsigned)std::max(1LL, std::min((long long)sms * per_sm, (items + warps_per_block - 1) / warps_per_block)),
+               1, 1);
+  } else {
+    grd.z = slices;
+  }
 #define RB_LAUNCH(NEE_, MS_) \
-  launch_ms<NEE_, MS_>(minb, grd, blk, sm, st, ds->view, G, P, acc, comp, part, counts, counters)
+  launch_ms<NEE_, MS_>(minb, grd, blk, sm, st, ds->view, G, P, acc, comp, part, counts, counters, fetch, slices)
   cudaEvent_t t0 = g_ktimer_on.load(std::memory_order_relaxed) ? ktimer_mark(st) : nullptr;
   if (G.nee) {
     if (ms == RB_MS_DIFFUSE) RB_LAUNCH(true, RB_MS_DIFFUSE);
@@ -887,14 +1021,12 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   }
   g_launches++;
   bool ok = cuda_ok(cudaGetLastError(), "k_render launch");
-  if (part) {
-    if (ok) {
-      k_fold_slices<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(acc, comp, part, (int)npix, slices - 1);
-      g_launches++;
-      ok = cuda_ok(cudaGetLastError(), "k_fold_slices launch");
-    }
-    cudaFreeAsync(part, st);
+  if (part && ok) {
+    k_fold_slices<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(acc, comp, part, (int)npix, slices - 1);
+    g_launches++;
+    ok = cuda_ok(cudaGetLastError(), "k_fold_slices launch");
   }
+  if (scratch) cudaFreeAsync(scratch, st);
   return ok ? RB_OK : RB_ERR_CUDA;
 }
 

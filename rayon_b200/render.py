@@ -64,9 +64,24 @@ def get_opts() -> RenderOpts:
     return o
 
 
+_SCHEDULES = {"auto": 0, "grid": 1, "fetch": 2}
+
+
 def set_opts(nee: bool | None = None, kahan: bool | None = None, seed: int | None = None,
-             block: tuple | None = None) -> None:
+             block: tuple | None = None, blocks_per_sm: int | None = None, slices: int | None = None,
+             schedule: str | None = None) -> None:
+    """Render options of the per-pixel kernel (rb_render_opts). blocks_per_sm:
+    register budget in resident 256-thread blocks (0 = tuned); slices: sample
+    slices per pixel (0 = automatic); schedule: "grid", "fetch" (persistent
+    warps taking 8x4-pixel tiles from a counter) or "auto" (the scene's tuned
+    schedule)."""
     o = get_opts()
+    if blocks_per_sm is not None:
+        o.reserved[0] = int(blocks_per_sm)
+    if slices is not None:
+        o.reserved[1] = int(slices)
+    if schedule is not None:
+        o.reserved[2] = _SCHEDULES[schedule]
     if nee is not None:
         o.nee = int(nee)
     if kahan is not None:

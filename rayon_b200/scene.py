@@ -221,13 +221,17 @@ class SceneDescription:
 
     # --- device --------------------------------------------------------------------
     def upload(self, quantized: bool = False, use_bvh: bool = True, stream=None, layout: str = "as_built",
-               max_leaf: int = 0, tune_depth: int = 0, probe=None, traversal_budget: int = 0) -> "DeviceScene":
+               max_leaf: int = 0, tune_depth: int = 0, probe=None, traversal_budget: int = 0,
+               wide: bool = True) -> "DeviceScene":
         """layout: "as_built" (the built BVH; bit-exact primary hits), "autotune"
         (fastest of linear / groups of 8, 16 / leaf 1, 2, 4, 8 on a probe render),
         "linear", "leaf" (rebuilt with max_leaf), "groups" (the built BVH's subtrees of
-        at most max_leaf primitives tested in order, no traversal stack)."""
+        at most max_leaf primitives tested in order, no traversal stack).
+        wide: the render kernels traverse a 4-wide copy of the tree (default); False
+        keeps the binary tree only."""
         o = UploadOpts()
         o.quantized_bvh = int(quantized)
+        o.wide_bvh = 1 if wide else -1
         o.use_bvh = int(use_bvh)
         o.layout = {"as_built": 0, "autotune": 1, "linear": 2, "leaf": 3, "groups": 4}[layout]
         o.max_leaf = int(max_leaf)

@@ -186,6 +186,33 @@ def test_autotuned_layout_renders_the_same(cuda, name):
 
 @pytest.mark.parametrize("name", ["cornell", "mixed_materials", "one_weekend", "small_icospheres"])
 @pytest.mark.parametrize("nee", [False, True])
+def test_wide_bvh_renders_the_same(cuda, name, nee):
+    # the 4-wide copy holds the binary tree's own child boxes and leaves: the
+    # same closest hits up to exact-t ties, so the same paths; primary hits
+    # (exact-order traversal) stay on the binary tree and are identical
+    spec, spp = _cases()[name]
+    w, h = spec.width, spec.height
+    sc = spec.to_scene()
+    sc.build_bvh()
+    fr = spec.camera.frame(w, h)
+    b_ds = sc.upload(wide=False)
+    w_ds = sc.upload()
+    assert w_ds.nbytes > b_ds.nbytes
+    np.testing.assert_array_equal(render.primary_hits(b_ds, fr, w, h), render.primary_hits(w_ds, fr, w, h))
+    a, ca = render.render_accumulate(b_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof,
+                                     nee=nee, counters=True)
+    b, cb = render.render_accumulate(w_ds, fr, w, h, spp, spec.depth, background=spec.background, dof=spec.dof,
+                                     nee=nee, counters=True)
+    assert int(cb[2]) == 0  # no stack overflow on the wide tree
+    bad = (np.abs(a - b) > 1e-3 * (1 + np.abs(a)) * spp).any(axis=2)
+    assert bad.mean() < 0.01, bad.mean()
+    np.testing.assert_allclose(a.mean((0, 1)), b.mean((0, 1)), rtol=1e-2, atol=1e-4)
+    for d in (b_ds, w_ds):
+        d.free()
+
+
+@pytest.mark.parametrize("name", ["cornell", "mixed_materials", "one_weekend", "small_icospheres"])
+@pytest.mark.parametrize("nee", [False, True])
 def test_wavefront_engine_paired_with_per_pixel_kernel(cuda, name, nee):
     spec, spp = _cases()[name]
     w, h = spec.width, spec.height
