@@ -492,11 +492,21 @@ __device__ __forceinline__ void qnode_visit(const SceneView &S, const RayPre &rp
   f3v = make_int4((int)b.z, (int)b.w, (int)((a.x & 1u) | ((a.y & 1u) << 1)), 0);
 }
 
+// Node layout a traversal reads. RB_NODES_ANY decides per scene at run time
+// (the 4-wide copy when SceneView::wnodes is set); RB_NODES_BINARY and
+// RB_NODES_WIDE fix it at compile time, so that a kernel specialised for one
+// layout carries neither the other's code nor its register pressure (the
+// wide visit holds 112 B of node words at once: compiled into the diffuse
+// class's per-pixel kernel it raised the spills around the traversal from 156
+// to 280 bytes per thread, and Cornell, which never runs it, lost 4 %). A
+// kernel specialised for RB_NODES_WIDE runs only on scenes that have wnodes.
+enum { RB_NODES_ANY = 0, RB_NODES_BINARY = 1, RB_NODES_WIDE = 2 };
+
 static __device__ bool sdf_field_march(const SceneView &S, const Ray &r, float tmin, float tmax, SdfCand &c,
                                        float &t, f3 &n, int &mat);
 
 // Closest hit in [tmin, tmax]. ANY: stop at the first hit (shadow rays).
-template <bool ANY, int MS, bool SPEC, class Sink = SdfCand>
+template <bool ANY, int MS, bool SPEC, class Sink = SdfCand, int NODES = RB_NODES_ANY>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                              uint32_t &overflow, Sink *cand);
 
@@ -508,13 +518,13 @@ __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray,
 #ifndef RB_SPEC_TRAVERSAL
 #define RB_SPEC_TRAVERSAL 1
 #endif
-template <bool ANY, int MS, bool SPEC = false>
+template <bool ANY, int MS, bool SPEC = false, int NODES = RB_NODES_ANY>
 __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                          uint32_t &overflow) {
   if (MS >= 4 && S.sdf_k > 0.0f && S.num_sdf > 0) {
     SdfCand cand;
     cand.n = 0;
-    HitInfo h = trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, &cand);
+    HitInfo h = trace_bvh<ANY, MS, SPEC, SdfCand, NODES>(S, ray, tmin, tmax, st, overflow, &cand);
     if (ANY && h.prim >= 0) return h;
     if (cand.n > 0) {
       float ts;
@@ -529,17 +539,17 @@ __device__ __forceinline__ HitInfo trace(const SceneView &S, const Ray &ray, flo
     }
     return h;
   }
-  return trace_bvh<ANY, MS, SPEC>(S, ray, tmin, tmax, st, overflow, static_cast<SdfCand *>(nullptr));
+  return trace_bvh<ANY, MS, SPEC, SdfCand, NODES>(S, ray, tmin, tmax, st, overflow, static_cast<SdfCand *>(nullptr));
 }
 
-template <bool ANY, int MS, class Sink>
+template <bool ANY, int MS, class Sink, int NODES>
 __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                             uint32_t &overflow, Sink *cand);
 
-template <bool ANY, int MS, bool SPEC, class Sink>
+template <bool ANY, int MS, bool SPEC, class Sink, int NODES>
 __device__ __forceinline__ HitInfo trace_bvh(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                              uint32_t &overflow, Sink *cand) {
-  if (SPEC && S.use_bvh) return trace_ww<ANY, MS, Sink>(S, ray, tmin, tmax, st, overflow, cand);
+  if (SPEC && S.use_bvh) return trace_ww<ANY, MS, Sink, NODES>(S, ray, tmin, tmax, st, overflow, cand);
   HitInfo h;
   h.t = tmax;
   h.prim = -1;
@@ -733,7 +743,7 @@ __device__ __forceinline__ int pop_next(Stack &st, float closest) {
   return RB_TRAV_DONE;
 }
 
-template <bool ANY, int MS, class Sink>
+template <bool ANY, int MS, class Sink, int NODES>
 __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, float tmin, float tmax, Stack &st,
                                             uint32_t &overflow, Sink *cand) {
   HitInfo h;
@@ -746,7 +756,7 @@ __device__ __forceinline__ HitInfo trace_ww(const SceneView &S, const Ray &ray, 
                closest, te))
     return h;
   st.sp = 0;
-  const bool wide = S.wnodes != nullptr;
+  const bool wide = NODES == RB_NODES_WIDE || (NODES == RB_NODES_ANY && S.wnodes != nullptr);
   int node = wide ? S.wide_root : S.root_ref;
   int leaf = RB_TRAV_DONE;  // postponed leaf
   // every interior node and every leaf is visited at most once, so this

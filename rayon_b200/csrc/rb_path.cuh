@@ -39,11 +39,11 @@ __device__ __forceinline__ Ray camera_ray(const FrameF &P, const Globals &G, int
 
 // One path segment: trace, shade, NEE, Russian roulette. Returns true when the
 // path ended (radiance complete in L).
-template <bool NEE, int MS>
+template <bool NEE, int MS, int NODES = RB_NODES_ANY>
 __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &G, Stack &st, uint32_t &ovf, Ray &ray,
                                              f3 &thr, f3 &L, int &bounce, float &prev_pdf, uint32_t key,
                                              int max_depth) {
-  const HitInfo h = trace<false, MS, RB_SPEC_TRAVERSAL>(S, ray, 0.001f, FLT_MAX, st, ovf);
+  const HitInfo h = trace<false, MS, RB_SPEC_TRAVERSAL, NODES>(S, ray, 0.001f, FLT_MAX, st, ovf);
   if (h.prim == -1) {  // miss (-2 is a hit on the smooth SDF field)
     if (G.background_intensity != 0.0f) L = L + thr * sky(ray.d) * G.background_intensity;
     return true;
@@ -88,7 +88,7 @@ __device__ __forceinline__ bool path_segment(const SceneView &S, const Globals &
           Ray sr;
           sr.o = o;
           sr.d = wi;
-          const HitInfo sh = trace<true, MS, RB_SPEC_TRAVERSAL>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
+          const HitInfo sh = trace<true, MS, RB_SPEC_TRAVERSAL, NODES>(S, sr, 0.001f, dist * (1.0f - 1e-4f), st, ovf);
           if (sh.prim == -1) {  // unoccluded
             const float pl = d2 / (cl * S.light_area);
             const float pb = cs * (1.0f / RB_PI);

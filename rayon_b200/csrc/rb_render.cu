@@ -17,6 +17,7 @@
 #include "host_scene.hpp"
 #include "rb_internal.hpp"
 #include "rb_path.cuh"
+#include "rb_render_kernel.cuh"
 
 using namespace rbd;
 
@@ -502,169 +503,6 @@ __global__ void __launch_bounds__(256) k_primary(const RB_GRID_CONST SceneView S
   if (tout) tout[pix] = h.prim >= 0 ? h.t : -1.0f;
 }
 
-// One pixel's sample slice z of nz: the pixel's samples of the slice back to
-// back in one flattened loop (one path segment per iteration). Adds the
-// thread's segments and paths to segs and paths.
-template <bool NEE, int MS>
-__device__ __forceinline__ void render_pixel_slice(const SceneView &S, const Globals &G, const FrameF &P, int x, int y,
-                                                   int z, int nz, int2 *smem, int tid, int threads,
-                                                   float4 *__restrict__ acc, float4 *__restrict__ comp,
-                                                   float4 *__restrict__ part, int *__restrict__ counts,
-                                                   unsigned long long *__restrict__ counters,
-                                                   unsigned long long &segs, unsigned long long &paths) {
-  const bool inside = x < P.width && y < P.height;
-  const int pix = inside ? y * P.width + x : 0;
-  int have = 0;
-  bool work = inside;
-  if (work && counts) {
-    have = counts[pix];
-    if (have < 0) work = false;  // converged (sign bit, render_acc_kernel.cu:165-170)
-  }
-  if (work) {
-    Stack st;
-    stack_init(st, smem, tid, threads, S.short_stack);
-    uint32_t ovf = 0;
-    // sample slice z of nz (small frames split their samples so that the
-    // launch fills the GPU): slice 0 adds into the pixel's sums, the others
-    // leave partial sums in part for k_fold_slices
-    const int s_begin = (int)((long long)P.samples * z / nz);
-    const int s_end = (int)((long long)P.samples * (z + 1) / nz);
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    if (z == 0) {
-      const float4 a0 = acc[pix];
-      sx = a0.x; sy = a0.y; sz = a0.z;
-      if (comp) {
-        const float4 c0 = comp[pix];
-        cx = c0.x; cy = c0.y; cz = c0.z;
-      }
-    }
-    float lum_before = 0.0f;
-    if (counts && have > 0) {
-      const float inv = 1.0f / (float)have;
-      lum_before = 0.299f * sx * inv + 0.587f * sy * inv + 0.114f * sz * inv;
-    }
-    int s = s_begin, bounce = 0;
-    bool alive = false;
-    Ray ray;
-    f3 thr(1.f, 1.f, 1.f), L(0.f, 0.f, 0.f);
-    uint32_t key = 0;
-    float prev_pdf = 0.0f;
-    const int nsamples = P.max_depth > 0 ? s_end : 0;  // depth 0: no bounce, black (ray_color's empty loop)
-    while (true) {
-      if (!alive) {
-        if (s >= nsamples) break;
-        key = rb_path_key(P.seed, P.salt, (uint32_t)pix, (uint32_t)(P.sample_base + s));
-        ++s;
-        ray = camera_ray(P, G, x, y, key);
-        thr = f3(1.f, 1.f, 1.f);
-        L = f3(0.f, 0.f, 0.f);
-        bounce = 0;
-        prev_pdf = 0.0f;
-        alive = true;
-      }
-      ++segs;
-      if (path_segment<NEE, MS>(S, G, st, ovf, ray, thr, L, bounce, prev_pdf, key, P.max_depth)) {
-        if (comp) {
-          kahan_add(sx, cx, L.x);
-          kahan_add(sy, cy, L.y);
-          kahan_add(sz, cz, L.z);
-        } else {
-          sx += L.x; sy += L.y; sz += L.z;
-        }
-        alive = false;
-      }
-    }
-    if (z == 0) {
-      acc[pix] = make_float4(sx, sy, sz, 0.0f);
-      if (comp) comp[pix] = make_float4(cx, cy, cz, 0.0f);
-    } else {
-      part[(size_t)(z - 1) * P.width * P.height + pix] = make_float4(sx - cx, sy - cy, sz - cz, 0.0f);
-    }
-    if (counts) {  // convergence test (render_acc_kernel.cu:241-271); counts are never split
-      const int nc = have + P.samples;
-      if (nc >= P.min_adaptive) {
-        const float inv = 1.0f / (float)nc;
-        const float lum_after = 0.299f * sx * inv + 0.587f * sy * inv + 0.114f * sz * inv;
-        const float rel = fabsf(lum_after - lum_before) / fmaxf(lum_after, 0.001f);
-        counts[pix] = rel < P.adaptive_threshold ? -nc : nc;
-      } else {
-        counts[pix] = nc;
-      }
-    }
-    if (counters && ovf) atomicAdd(counters + 2, (unsigned long long)ovf);
-    paths += (unsigned long long)(s_end - s_begin);
-  }
-}
-
-// Per-pixel progressive kernel: one thread owns one pixel for the launch and
-// runs its samples back to back in a single flattened loop (one path segment
-// per iteration), so a lane whose path ended starts its next sample at once
-// instead of idling until the warp's longest path finishes.
-//
-// Two schedules of the same work. Grid mode (fetch == nullptr): one thread per
-// pixel of a 2-D grid of bx x by blocks, sample slice blockIdx.z of gridDim.z.
-// Fetch mode: a persistent grid of 1-D blocks sized to the SMs' resident
-// capacity; each warp takes work items (a tile of 8 x 4 pixels in one sample
-// slice of `nslices`) from the counter *fetch until they run out, so a warp
-// whose tile finished early starts the next one instead of idling until its
-// block's other warps and the launch's last wave finish. Items run slice-major,
-// then tile rows, so concurrent warps work on neighbouring tiles. A pixel's
-// slice is computed by one thread in sample order either way: the sums are the
-// same bit for bit.
-#define RB_TILE_W 8
-#define RB_TILE_H 4
-template <bool NEE, int MS, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_render(const RB_GRID_CONST SceneView S,
-                                                      const RB_GRID_CONST Globals G,
-                                                      const RB_GRID_CONST FrameF P, float4 *__restrict__ acc,
-                                                float4 *__restrict__ comp, float4 *__restrict__ part,
-                                                int *__restrict__ counts, unsigned long long *__restrict__ counters,
-                                                int *__restrict__ fetch, int nslices) {
-  extern __shared__ int2 smem[];
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int threads = blockDim.x * blockDim.y;
-  const int lane = tid & 31;
-  const int tiles_x = (P.width + RB_TILE_W - 1) / RB_TILE_W;
-  const int tiles = tiles_x * ((P.height + RB_TILE_H - 1) / RB_TILE_H);
-  const long long items = fetch ? (long long)tiles * nslices : 0;
-  unsigned long long segs = 0, paths = 0;
-  for (;;) {
-    int x, y, z, nz;
-    if (fetch) {
-      int it = 0;
-      if (lane == 0) it = atomicAdd(fetch, 1);
-      it = __shfl_sync(0xffffffffu, it, 0);
-      if (it >= items) break;
-      z = it / tiles;
-      const int tile = it - z * tiles;
-      const int ty = tile / tiles_x;
-      x = (tile - ty * tiles_x) * RB_TILE_W + (lane & (RB_TILE_W - 1));
-      y = ty * RB_TILE_H + lane / RB_TILE_W;
-      nz = nslices;
-    } else {
-      x = blockIdx.x * blockDim.x + threadIdx.x;
-      y = blockIdx.y * blockDim.y + threadIdx.y;
-      z = blockIdx.z;
-      nz = gridDim.z;
-    }
-    render_pixel_slice<NEE, MS>(S, G, P, x, y, z, nz, smem, tid, threads, acc, comp, part, counts, counters, segs,
-                                paths);
-    if (!fetch) break;
-  }
-  if (counters) {
-    // warp-aggregated segment and path counts
-    for (int o = 16; o > 0; o >>= 1) {
-      segs += __shfl_down_sync(0xffffffffu, segs, o);
-      paths += __shfl_down_sync(0xffffffffu, paths, o);
-    }
-    if (lane == 0) {
-      atomicAdd(counters, segs);
-      atomicAdd(counters + 1, paths);
-    }
-  }
-}
-
 // Adds the partial sums of sample slices 1..parts into the pixel sums, in
 // slice order (Kahan-compensated when comp is given).
 __global__ void k_fold_slices(float4 *__restrict__ acc, float4 *__restrict__ comp, const float4 *__restrict__ part,
@@ -811,33 +649,6 @@ static void default_block(int ms, int &bx, int &by) {
   bx = by = 8;  // 8x8 tiles: a warp's rays stay close together
 }
 
-template <bool NEE, int MS>
-static void launch_ms(int minb, dim3 grd, dim3 blk, size_t sm, cudaStream_t st, const SceneView &S, const Globals &G,
-                      const FrameF &P, float4 *acc, float4 *comp, float4 *part, int *counts,
-                      unsigned long long *counters, int *fetch, int nslices) {
-  switch (minb) {
-    case 1: k_render<NEE, MS, 1><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
-    case 3: k_render<NEE, MS, 3><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
-    case 4: k_render<NEE, MS, 4><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
-    default: k_render<NEE, MS, 2><<<grd, blk, sm, st>>>(S, G, P, acc, comp, part, counts, counters, fetch, nslices); break;
-  }
-}
-
-// Resident blocks per SM of k_render<NEE, MS, minb> at `threads` threads and
-// `sm` bytes of dynamic shared memory (the persistent grid of fetch mode).
-template <bool NEE, int MS>
-static int resident_blocks(int minb, int threads, size_t sm) {
-  int n = 0;
-  cudaError_t e;
-  switch (minb) {
-    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 1>, threads, sm); break;
-    case 3: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 3>, threads, sm); break;
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 4>, threads, sm); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_render<NEE, MS, 2>, threads, sm); break;
-  }
-  return e == cudaSuccess && n > 0 ? n : 1;
-}
-
 // Stream-ordered scratch of the sample slices: a private memory pool per
 // device that keeps its memory between calls (the default pool returns freed
 // memory at every synchronisation, and mapping it again stalls the stream).
@@ -890,31 +701,33 @@ static cudaEvent_t ktimer_mark(cudaStream_t st) {
 // Fetch mode's block size (two warps) and its resident blocks per SM per
 // kernel instance (cached: the occupancy query is a driver call).
 #define RB_FETCH_THREADS 64
-static int fetch_resident_blocks(int ms, bool nee, int minb, int sm) {
+// One k_render launch (launch == true) or its resident-block query, on the
+// instances of the scene's node layout.
+static int k_render_for(const DeviceScene *ds, bool launch, bool nee, int minb, dim3 grd, dim3 blk, size_t sm,
+                        cudaStream_t st, const Globals &G, const FrameF &P, float4 *acc, float4 *comp, float4 *part,
+                        int *counts, unsigned long long *counters, int *fetch, int nslices) {
+  const SceneView &S = ds->view;
+  if (S.use_bvh && S.wnodes)
+    return k_render_dispatch_wide(launch, nee, ds->ms, minb, grd, blk, sm, st, S, G, P, acc, comp, part, counts,
+                                  counters, fetch, nslices);
+  return k_render_dispatch<RB_NODES_BINARY>(launch, nee, ds->ms, minb, grd, blk, sm, st, S, G, P, acc, comp, part,
+                                            counts, counters, fetch, nslices);
+}
+
+static int fetch_resident_blocks(const DeviceScene *ds, bool nee, int minb, int sm) {
   static std::mutex mu;
   static std::map<std::tuple<int, int, int, int, int>, int> cache;
   int dev = 0;
   cudaGetDevice(&dev);
-  const auto key = std::make_tuple(dev, ms * 2 + (nee ? 1 : 0), minb, sm, (int)RB_FETCH_THREADS);
+  const int wide = ds->view.use_bvh && ds->view.wnodes ? 1 : 0;
+  const auto key = std::make_tuple(dev, (ds->ms * 2 + (nee ? 1 : 0)) * 2 + wide, minb, sm, (int)RB_FETCH_THREADS);
   {
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
   }
-  int n = 1;
-#define RB_RES(NEE_, MS_) n = resident_blocks<NEE_, MS_>(minb, RB_FETCH_THREADS, (size_t)sm)
-  if (nee) {
-    if (ms == RB_MS_DIFFUSE) RB_RES(true, RB_MS_DIFFUSE);
-    else if (ms == RB_MS_CLASSIC) RB_RES(true, RB_MS_CLASSIC);
-    else if (ms == RB_MS_FULL) RB_RES(true, RB_MS_FULL);
-    else RB_RES(true, RB_MS_SDF);
-  } else {
-    if (ms == RB_MS_DIFFUSE) RB_RES(false, RB_MS_DIFFUSE);
-    else if (ms == RB_MS_CLASSIC) RB_RES(false, RB_MS_CLASSIC);
-    else if (ms == RB_MS_FULL) RB_RES(false, RB_MS_FULL);
-    else RB_RES(false, RB_MS_SDF);
-  }
-#undef RB_RES
+  const int n = k_render_for(ds, false, nee, minb, dim3(1), dim3(RB_FETCH_THREADS), (size_t)sm, nullptr, Globals(),
+                             FrameF(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0);
   std::lock_guard<std::mutex> lk(mu);
   cache[key] = n;
   return n;
@@ -955,12 +768,14 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // A frame with fewer pixels than four times the GPU's resident threads
-  // splits its samples into up to 8 slices (grid z), so that the launch keeps
-  // the GPU full to its end (measured on B200: 400x225 x 32 spp 1.99 -> 1.13 ms,
-  // 512x512 x 256 spp 16.4 -> 15.1 ms); slices 1.. leave partial sums in a
-  // stream-ordered scratch buffer that k_fold_slices adds in slice order. Not
-  // with adaptive counts (their test needs each pixel's whole batch in one
-  // thread).
+  // splits its samples into up to 8 slices (grid z in the grid schedule), so
+  // that the launch keeps the GPU full to its end (measured on B200: 400x225 x
+  // 32 spp 1.99 -> 1.13 ms, 512x512 x 256 spp 16.4 -> 15.1 ms); slices 1..
+  // leave partial sums in a stream-ordered scratch buffer that k_fold_slices
+  // adds in slice order. Splitting further (up to 16 times the resident
+  // threads in pixel slices) ran slower on both (Cornell 512x512 x 51 spp
+  // 3.35 -> 3.72 ms). Not with adaptive counts (their test needs each
+  // pixel's whole batch in one thread).
   const long long npix = (long long)P.width * P.height;
   int slices = 1;
   if (!counts && P.samples > 1 && P.max_depth > 0) {
@@ -991,28 +806,15 @@ int launch_render(const DeviceScene *ds, const Globals &G, const FrameF &P, floa
     cudaMemsetAsync(fetch, 0, sizeof(int), st);
     const long long items = (long long)((P.width + RB_TILE_W - 1) / RB_TILE_W) *
                             ((P.height + RB_TILE_H - 1) / RB_TILE_H) * slices;
-    const long long per_sm = fetch_resident_blocks(ds->ms, G.nee != 0, minb, (int)sm);
+    const long long per_sm = fetch_resident_blocks(ds, G.nee != 0, minb, (int)sm);
     const long long warps_per_block = RB_FETCH_THREADS / 32;
     grd = dim3((unsigned)std::max(1LL, std::min((long long)sms * per_sm, (items + warps_per_block - 1) / warps_per_block)),
                1, 1);
   } else {
     grd.z = slices;
   }
-#define RB_LAUNCH(NEE_, MS_) \
-  launch_ms<NEE_, MS_>(minb, grd, blk, sm, st, ds->view, G, P, acc, comp, part, counts, counters, fetch, slices)
   cudaEvent_t t0 = g_ktimer_on.load(std::memory_order_relaxed) ? ktimer_mark(st) : nullptr;
-  if (G.nee) {
-    if (ms == RB_MS_DIFFUSE) RB_LAUNCH(true, RB_MS_DIFFUSE);
-    else if (ms == RB_MS_CLASSIC) RB_LAUNCH(true, RB_MS_CLASSIC);
-    else if (ms == RB_MS_FULL) RB_LAUNCH(true, RB_MS_FULL);
-    else RB_LAUNCH(true, RB_MS_SDF);
-  } else {
-    if (ms == RB_MS_DIFFUSE) RB_LAUNCH(false, RB_MS_DIFFUSE);
-    else if (ms == RB_MS_CLASSIC) RB_LAUNCH(false, RB_MS_CLASSIC);
-    else if (ms == RB_MS_FULL) RB_LAUNCH(false, RB_MS_FULL);
-    else RB_LAUNCH(false, RB_MS_SDF);
-  }
-#undef RB_LAUNCH
+  k_render_for(ds, true, G.nee != 0, minb, grd, blk, sm, st, G, P, acc, comp, part, counts, counters, fetch, slices);
   if (t0) {
     cudaEvent_t t1 = ktimer_mark(st);
     std::lock_guard<std::mutex> lk(g_ktimer_mu);
@@ -1414,22 +1216,29 @@ void rb_set_render_opts(const rb_render_opts *o) {
   if (o) g_opts = *o;
 }
 
+// Buffers this library handed out came from its memory pool and go back to it
+// in stream order (legacy default stream, as the reference's cudaFree is
+// ordered after all prior work); anything else is released with cudaFree.
 void freeDeviceRandomStates(void *p) {
   if (!p) return;
+  bool ours = false;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_rng_ctx.erase(p);
+    ours = g_rng_ctx.erase(p) > 0;
   }
-  cudaFree(p);
+  if (ours) cudaFreeAsync(p, 0);
+  else cudaFree(p);
 }
 
 void freeDeviceAccumBuffer(void *p) {
   if (!p) return;
+  bool ours = false;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    g_accum_bytes.erase(p);
+    ours = g_accum_bytes.erase(p) > 0;
   }
-  cudaFree(p);
+  if (ours) cudaFreeAsync(p, 0);
+  else cudaFree(p);
 }
 
 void resetDeviceAccumBuffer(void *p, int num_pixels) {
@@ -1502,9 +1311,15 @@ unsigned long long renderPixelsCUDAAccumulative(
   cudaStream_t st = 0;
   // RNG context: the per-path streams are counter based; the context keeps
   // the index of the next sample so that successive calls draw new samples.
+  // Both allocations come from the per-device pool that keeps its memory, so a
+  // renderer that allocates and frees them for every frame (RendererCUDA::render)
+  // pays neither cudaMalloc nor the device-wide synchronisation of cudaFree
+  // (measured: 2.4 ms more on a frame's first call, frees of 0.4 to 19 ms).
+  cudaMemPool_t pool = scratch_pool();
+  if (!pool) return 0ull;
   if (*d_rand_states_ptr == nullptr) {
     void *p = nullptr;
-    if (!cuda_ok(cudaMalloc(&p, 256), "cudaMalloc(rng context)")) return 0ull;
+    if (!cuda_ok(cudaMallocFromPoolAsync(&p, 256, pool, st), "rng context")) return 0ull;
     *d_rand_states_ptr = p;
     std::lock_guard<std::mutex> lk(g_mu);
     g_rng_ctx[p] = 0;
@@ -1512,7 +1327,7 @@ unsigned long long renderPixelsCUDAAccumulative(
   float4 *acc = nullptr;
   const size_t nb = (size_t)n * sizeof(float4);
   if (*d_accum_buffer_ptr == nullptr) {
-    if (!cuda_ok(cudaMalloc((void **)&acc, 2 * nb), "cudaMalloc(accum)")) return 0ull;
+    if (!cuda_ok(cudaMallocFromPoolAsync((void **)&acc, 2 * nb, pool, st), "accumulation buffer")) return 0ull;
     *d_accum_buffer_ptr = acc;
     {
       std::lock_guard<std::mutex> lk(g_mu);
