@@ -288,6 +288,14 @@ int64_t rb_scene_device_bytes(const rb_cuda_scene *scene);
  * the counter after reading it. */
 int rb_scene_traversal_faults(const rb_cuda_scene *scene, uint64_t *count, int reset);
 
+/* Host-only check of the 4-wide copy of a built scene's BVH (no device
+ * needed): builds the upload layout on the host and verifies that every
+ * binary-tree leaf is reached exactly once, every wide node once, child refs
+ * stay in range and each child node's boxes lie inside its slot's box. out:
+ * [wide nodes, leaves reached, binary-tree leaves, depth]. RB_OK when
+ * consistent. */
+int rb_scene_check_wide(const rb_scene_desc *s, int64_t out[4]);
+
 /* Primary hits: pixel-centre rays (no jitter, no DOF), closest hit over the
  * device BVH; ids[w*h] = leaf-order geometry index or -1; t may be NULL.
  * ids / t are DEVICE pointers. */
@@ -421,7 +429,9 @@ typedef struct rb_server_opts {
   int64_t memory_budget_bytes;  /* HBM admission budget: accumulation + frame buffers */
   int max_active_jobs;          /* slots of the batched launch (<= 1024) */
   int64_t paths_per_iteration;  /* work quantum of one batched launch */
-  int max_spp_per_iteration;    /* per-job cap of samples per pixel per launch */
+  int max_spp_per_iteration;    /* per-job cap of samples per pixel per launch of the batched
+                                   kernel (jobs on the per-frame kernel take what the path
+                                   quantum allows) */
   int use_graph;                /* 1: each iteration is a CUDA graph launch */
   int frames_every;             /* > 0: write each active job's u8 frame every N iterations */
   int occupancy;                /* resident 256-thread blocks per SM (0 = tuned) */

@@ -143,6 +143,7 @@ _sig("rb_scene_upload", vp, vp, C.POINTER(UploadOpts), vp)
 _sig("rb_scene_free_device", None, vp)
 _sig("rb_scene_device_bytes", C.c_int64, vp)
 _sig("rb_scene_traversal_faults", C.c_int, vp, c_uint64_p, C.c_int)
+_sig("rb_scene_check_wide", C.c_int, vp, C.POINTER(C.c_int64))
 _sig("rb_scene_layout_info", C.c_int, vp, c_int32_p, c_int32_p, c_float_p)
 
 

@@ -1526,6 +1526,92 @@ int rb_scene_traversal_faults(const rb_cuda_scene *scene, uint64_t *count, int r
   return RB_OK;
 }
 
+int rb_scene_check_wide(const rb_scene_desc *s, int64_t out[4]) {
+  if (!s || !out) {
+    set_error("rb_scene_check_wide: null argument");
+    return RB_ERR_INVALID_ARG;
+  }
+  const HostScene &hs = host_scene_of(s);
+  rb_upload_opts o;
+  std::memset(&o, 0, sizeof o);
+  o.use_bvh = 1;
+  HostLayout L;
+  try {
+    if (!build_device_layout(hs, o, L)) return RB_ERR_INVALID_ARG;
+  } catch (const std::exception &e) {
+    set_error(std::string("rb_scene_check_wide: ") + e.what());
+    return RB_ERR_INVALID_ARG;
+  }
+  for (int k = 0; k < 4; ++k) out[k] = 0;
+  if (!L.use_bvh) return RB_OK;
+  // the binary tree's leaves, by first primitive
+  std::unordered_map<int, int> leaves;  // first -> times reached in the wide tree
+  const size_t nbin = L.nodes.size() / 4;
+  auto note_leaf = [&](int r) { leaves.emplace(leaf_first(r), 0); };
+  if (ref_is_leaf(L.root_ref)) note_leaf(L.root_ref);
+  for (size_t i = 0; i < nbin; ++i) {
+    const int *wi = reinterpret_cast<const int *>(&L.nodes[4 * i + 3]);
+    for (int c = 0; c < 2; ++c)
+      if (ref_is_leaf(wi[c])) note_leaf(wi[c]);
+  }
+  out[2] = (int64_t)leaves.size();
+  const int64_t nwide = (int64_t)(L.wnodes.size() / 8);
+  out[0] = nwide;
+  if (nwide == 0) {  // a leaf root keeps the binary root
+    out[1] = ref_is_leaf(L.wide_root) ? 1 : 0;
+    return out[1] == out[2] ? RB_OK : RB_ERR_INVALID_ARG;
+  }
+  std::vector<std::pair<int, int>> todo{{L.wide_root, 1}};
+  std::vector<char> seen(nwide, 0);
+  int64_t reached = 0;
+  while (!todo.empty()) {
+    const auto [n, depth] = todo.back();
+    todo.pop_back();
+    if (n < 0 || n >= nwide || seen[n]) {
+      set_error("rb_scene_check_wide: wide node out of range or reached twice");
+      return RB_ERR_INVALID_ARG;
+    }
+    seen[n] = 1;
+    out[3] = std::max<int64_t>(out[3], depth);
+    const float *w = reinterpret_cast<const float *>(&L.wnodes[8 * (size_t)n]);
+    const int *r = reinterpret_cast<const int *>(&L.wnodes[8 * (size_t)n + 6]);
+    for (int c = 0; c < 4; ++c) {
+      if (!std::isfinite(w[c])) continue;  // empty slot
+      if (ref_is_leaf(r[c])) {
+        auto it = leaves.find(leaf_first(r[c]));
+        if (it == leaves.end() || it->second++ > 0) {
+          set_error("rb_scene_check_wide: a leaf missing from the binary tree or reached twice");
+          return RB_ERR_INVALID_ARG;
+        }
+        ++reached;
+        continue;
+      }
+      if (r[c] < 0 || r[c] >= nwide) {
+        set_error("rb_scene_check_wide: child ref out of range");
+        return RB_ERR_INVALID_ARG;
+      }
+      // the child's slot box bounds every box inside the child node
+      const float *cw = reinterpret_cast<const float *>(&L.wnodes[8 * (size_t)r[c]]);
+      for (int g = 0; g < 4; ++g) {
+        if (!std::isfinite(cw[g])) continue;
+        for (int k = 0; k < 3; ++k)
+          if (cw[8 * k + g] < w[8 * k + c] || cw[8 * k + 4 + g] > w[8 * k + 4 + c]) {
+            set_error("rb_scene_check_wide: a child box outside its slot box");
+            return RB_ERR_INVALID_ARG;
+          }
+      }
+      todo.push_back({r[c], depth + 1});
+    }
+  }
+  out[1] = reached;
+  for (int64_t i = 0; i < nwide; ++i)
+    if (!seen[i]) {
+      set_error("rb_scene_check_wide: unreachable wide node");
+      return RB_ERR_INVALID_ARG;
+    }
+  return reached == out[2] ? RB_OK : RB_ERR_INVALID_ARG;
+}
+
 int64_t rb_scene_device_bytes(const rb_cuda_scene *scene) {
   DeviceScene *ds = lookup_scene(scene);
   return ds ? (int64_t)ds->bytes : 0;

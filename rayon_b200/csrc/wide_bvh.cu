@@ -14,9 +14,13 @@
 // (interior: wide node index; leaf: the binary tree's leaf encoding) and a
 // padding word. An empty child slot has every bound at +inf, which the slab
 // test rejects for every ray (both slab distances are +inf or both -inf).
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <limits>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -50,61 +54,138 @@ void binary_children(const HostLayout &L, int ref, Child out[2]) {
   out[1].ref = wi[1];
 }
 
-}  // namespace
+// The up-to-four children of the wide node that replaces binary interior
+// node `bref`: its two children, then the interior child of largest surface
+// area opened until four are held or only leaves remain.
+int collapse(const HostLayout &L, int bref, Child ch[4]) {
+  int n = 2;
+  binary_children(L, bref, ch);
+  while (n < 4) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (int c = 0; c < n; ++c)
+      if (!rbd::ref_is_leaf(ch[c].ref) && area(ch[c]) > best_area) {
+        best = c;
+        best_area = area(ch[c]);
+      }
+    if (best < 0) break;
+    Child two[2];
+    binary_children(L, ch[best].ref, two);
+    ch[best] = two[0];
+    ch[n++] = two[1];
+  }
+  return n;
+}
 
-void build_wide(HostLayout &L) {
-  L.wnodes.clear();
-  L.wide_root = L.root_ref;
-  if (!L.use_bvh || L.nodes.empty() || rbd::ref_is_leaf(L.root_ref)) return;
-  const size_t nbin = L.nodes.size() / 4;
-  L.wnodes.reserve(8 * (nbin / 2 + 1));
+// Writes one wide node (8 words) with child refs `refs` (interior children
+// get their ref patched later where it is not known yet).
+void write_node(float4 *dst, const Child ch[4], int n, const int refs[4]) {
   const float inf = std::numeric_limits<float>::infinity();
-  auto alloc = [&]() {
-    const int slot = (int)(L.wnodes.size() / 8);
-    L.wnodes.resize(L.wnodes.size() + 8);
-    return slot;
-  };
-  std::vector<std::pair<int, int>> todo;  // (binary interior ref, wide slot)
-  L.wide_root = alloc();
-  todo.push_back({L.root_ref, L.wide_root});
+  float *w = reinterpret_cast<float *>(dst);
+  for (int c = 0; c < 4; ++c)
+    for (int k = 0; k < 3; ++k) {
+      w[8 * k + c] = c < n ? ch[c].lo[k] : inf;
+      w[8 * k + 4 + c] = c < n ? ch[c].hi[k] : inf;
+    }
+  int *wi = reinterpret_cast<int *>(dst + 6);
+  for (int c = 0; c < 4; ++c) wi[c] = refs[c];
+  for (int c = 4; c < 8; ++c) wi[c] = 0;
+}
+
+int *ref_slot(float4 *node, int lane) { return reinterpret_cast<int *>(node + 6) + lane; }
+
+// The wide subtree of binary interior node `bref` in depth-first order, its
+// root at local slot 0 and interior refs local to `out`.
+void build_subtree(const HostLayout &L, int bref, std::vector<float4> &out) {
+  std::vector<std::pair<int, int>> todo{{bref, 0}};
+  out.resize(8);
   while (!todo.empty()) {
-    const auto [bref, slot] = todo.back();
+    const auto [b, slot] = todo.back();
     todo.pop_back();
     Child ch[4];
-    int n = 2;
-    binary_children(L, bref, ch);
-    while (n < 4) {
-      int best = -1;
-      float best_area = -1.0f;
-      for (int c = 0; c < n; ++c)
-        if (!rbd::ref_is_leaf(ch[c].ref) && area(ch[c]) > best_area) {
-          best = c;
-          best_area = area(ch[c]);
-        }
-      if (best < 0) break;
-      Child two[2];
-      binary_children(L, ch[best].ref, two);
-      ch[best] = two[0];
-      ch[n++] = two[1];
-    }
+    const int n = collapse(L, b, ch);
     int refs[4] = {0, 0, 0, 0};
     for (int c = 0; c < n; ++c) {
       if (rbd::ref_is_leaf(ch[c].ref)) {
         refs[c] = ch[c].ref;
       } else {
-        refs[c] = alloc();  // children of a node sit next to each other
+        refs[c] = (int)(out.size() / 8);  // children of a node sit next to each other
+        out.resize(out.size() + 8);
         todo.push_back({ch[c].ref, refs[c]});
       }
     }
-    float *w = reinterpret_cast<float *>(&L.wnodes[8 * (size_t)slot]);
-    for (int c = 0; c < 4; ++c)
-      for (int k = 0; k < 3; ++k) {
-        w[8 * k + c] = c < n ? ch[c].lo[k] : inf;
-        w[8 * k + 4 + c] = c < n ? ch[c].hi[k] : inf;
-      }
-    int *wi = reinterpret_cast<int *>(&L.wnodes[8 * (size_t)slot + 6]);
-    for (int c = 0; c < 4; ++c) wi[c] = refs[c];
-    for (int c = 4; c < 8; ++c) wi[c] = 0;
+    write_node(&out[8 * (size_t)slot], ch, n, refs);
+  }
+}
+
+}  // namespace
+
+// The top of the tree is collapsed breadth-first on one thread until it has
+// at least 256 pending interior children; their subtrees are then built on
+// all host cores (each a depth-first block) and appended in order, their
+// interior refs shifted to the block's position (the nodes reached through
+// one top-level child stay contiguous, as in a single depth-first build).
+void build_wide(HostLayout &L) {
+  L.wnodes.clear();
+  L.wide_root = L.root_ref;
+  if (!L.use_bvh || L.nodes.empty() || rbd::ref_is_leaf(L.root_ref)) return;
+  struct Pending {
+    int bref, parent, lane;
+  };
+  std::vector<float4> top;
+  std::deque<Pending> q;
+  auto emit = [&](int bref) {
+    const int slot = (int)(top.size() / 8);
+    top.resize(top.size() + 8);
+    Child ch[4];
+    const int n = collapse(L, bref, ch);
+    int refs[4] = {0, 0, 0, 0};
+    for (int c = 0; c < n; ++c) {
+      if (rbd::ref_is_leaf(ch[c].ref)) refs[c] = ch[c].ref;
+      else q.push_back({ch[c].ref, slot, c});
+    }
+    write_node(&top[8 * (size_t)slot], ch, n, refs);
+    return slot;
+  };
+  L.wide_root = emit(L.root_ref);  // slot 0
+  while (!q.empty() && q.size() < 256) {
+    const Pending p = q.front();
+    q.pop_front();
+    const int slot = emit(p.bref);
+    *ref_slot(&top[8 * (size_t)p.parent], p.lane) = slot;
+  }
+  const std::vector<Pending> rest(q.begin(), q.end());
+  std::vector<std::vector<float4>> sub(rest.size());
+  {
+    const size_t threads = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 64);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+      for (size_t i = next++; i < rest.size(); i = next++) build_subtree(L, rest[i].bref, sub[i]);
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < threads && t < rest.size(); ++t) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+  }
+  std::vector<size_t> base(rest.size());
+  size_t total = top.size();
+  for (size_t i = 0; i < rest.size(); ++i) {
+    base[i] = total / 8;
+    total += sub[i].size();
+  }
+  L.wnodes.resize(total);
+  std::copy(top.begin(), top.end(), L.wnodes.begin());
+  for (size_t i = 0; i < rest.size(); ++i) {
+    *ref_slot(&L.wnodes[8 * (size_t)rest[i].parent], rest[i].lane) = (int)base[i];
+    float4 *dst = &L.wnodes[8 * base[i]];
+    std::copy(sub[i].begin(), sub[i].end(), dst);
+    const int shift = (int)base[i];
+    for (size_t k = 0; k < sub[i].size() / 8; ++k) {
+      const float *w = reinterpret_cast<const float *>(dst + 8 * k);
+      int *refs = reinterpret_cast<int *>(dst + 8 * k + 6);
+      for (int c = 0; c < 4; ++c)  // valid interior children: a finite bound, a non-leaf ref
+        if (std::isfinite(w[c]) && !rbd::ref_is_leaf(refs[c])) refs[c] += shift;
+    }
   }
 }
 

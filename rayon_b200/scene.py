@@ -199,6 +199,16 @@ class SceneDescription:
                                           ax.ctypes.data_as(c_uint8_p)), "export_bvh")
         return BVHExport(bounds, a, b, leaf, ax, int(lib.rb_scene_bvh_root(self._h)))
 
+    def check_wide(self) -> dict:
+        """Host-only consistency check of the 4-wide copy of the built BVH
+        (rb_scene_check_wide): raises on an inconsistency, returns the counts."""
+        out = np.zeros(4, np.int64)
+        st = lib.rb_scene_check_wide(self._h, out.ctypes.data_as(C.POINTER(C.c_int64)))
+        if st != 0:
+            raise RuntimeError(f"rb_scene_check_wide: {(lib.rb_last_error() or b'').decode()}")
+        return {"wide_nodes": int(out[0]), "leaves_reached": int(out[1]), "binary_leaves": int(out[2]),
+                "depth": int(out[3])}
+
     def export_order(self) -> np.ndarray:
         o = np.zeros(self.num_geometries, np.int64)
         if o.size:
