@@ -458,6 +458,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the equal-RMSE and serving sections")
     ap.add_argument("--serving-jobs", type=int, default=400,
                     help="jobs of the serving section's stream (2000 = the full specified stream, ~15 min)")
+    ap.add_argument("--serving-by-scene", action="store_true",
+                    help="serving section: also serve each scene's jobs alone (served/plain per scene)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case for ncu: same frame at 16 spp (two views at most), no e2e/baselines")
     args = ap.parse_args()
@@ -674,7 +676,7 @@ def main():
     res["mean_radiance"] = mean_rad
     if rank == 0 and world == 1 and args.workload == "cornell" and not args.small and not args.no_extras:
         for key, fn in (("equal_rmse", lambda: equal_rmse_section(t_ms, paths)),
-                        ("serving", lambda: serving_section(args.serving_jobs))):
+                        ("serving", lambda: serving_section(args.serving_jobs, by_scene=args.serving_by_scene))):
             try:
                 res[key] = fn()
             except Exception as e:  # noqa: BLE001
@@ -793,7 +795,7 @@ def reference_cuda(spec):
                     "e2e excludes its scene build and upload (scene_build_upload_s)"}
 
 
-def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False):
+def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False, by_scene: bool = False):
     """The serving mix: n_jobs Poisson arrivals at `rate` jobs/s (2000 in the
     specified stream) over the One-Weekend, Cornell, icosphere and SDF scenes,
     resolutions from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform
@@ -804,7 +806,9 @@ def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False
     (device seconds) and the loop on the wall clock; served: the batched
     serving loop with real-time arrivals (wall clock; device seconds from the
     server's own events); backlog (optional): the same jobs all queued at
-    once. Ratios are wall/wall and device/device."""
+    once. Ratios are wall/wall and device/device. by_scene: each scene's jobs
+    of the mix served alone as a backlog, against the same jobs' plain
+    launches (device time), so the gain is attributed scene by scene."""
     import torch
 
     from rayon_b200 import lib, render, scenes, serving
@@ -880,6 +884,29 @@ def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False
         srv.close()
         out_backlog = {"backlog_mpaths_s_wall": paths / wall_b / 1e6,
                        "backlog_mpaths_s_device": sb.paths / sb.device_seconds / 1e6 if sb.device_seconds else None}
+    by_scene_out = {}
+    if by_scene:
+        for i, nm in enumerate(names):
+            sel = [(r, j) for r, j in zip(reqs, mix) if j["scene"] == i]
+            if not sel:
+                continue
+            srv = serving.Server(paths_per_iteration=64 << 20, max_spp_per_iteration=64)
+            ids = [srv.add_scene(ds) for ds in dss]
+            for r, j in sel:
+                r.scene = ids[j["scene"]]
+                r.arrival_time = 0.0
+            tb = time.time()
+            srv.run_trace([r for r, _ in sel], realtime=False)
+            wall_s = time.time() - tb
+            ss = srv.stats()
+            srv.close()
+            by_scene_out[nm] = {"jobs": len(sel),
+                                "served_mpaths_s_device": scene_paths[i] / ss.device_seconds / 1e6
+                                if ss.device_seconds else None,
+                                "served_mpaths_s_wall": scene_paths[i] / wall_s / 1e6,
+                                "plain_mpaths_s_device": scene_paths[i] / scene_dev[i] / 1e6 if scene_dev[i] else None,
+                                "served_over_plain_device": scene_dev[i] / ss.device_seconds
+                                if ss.device_seconds else None}
     clk.__exit__(None, None, None)
     path_csv = clk.path
     runs = [("plain", (clk.t0, clk.t1)), ("served", clk_t)] + ([("backlog", clk_b)] if clk_b else [])
@@ -909,6 +936,8 @@ def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False
            "clocks": clocks,
            "note": "offered load exceeds one GPU's capacity, so latency is queue-dominated"}
     res.update(out_backlog)
+    if by_scene_out:
+        res["served_over_plain_by_scene"] = by_scene_out
     return res
 
 
