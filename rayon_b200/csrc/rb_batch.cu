@@ -327,6 +327,8 @@ struct Job {
   int error = 0;  // rb_status of a rejection
 };
 
+#define RB_PF_STREAMS 4
+
 struct Server {
   rb_server_opts o;
   cudaStream_t st = nullptr;
@@ -352,6 +354,12 @@ struct Server {
   // marks the iteration's uploads, ev_wf the end of its wavefront runs
   cudaStream_t st_wf = nullptr;
   cudaEvent_t ev_up = nullptr, ev_wf = nullptr;
+  // per-frame jobs of an iteration run round-robin on RB_PF_STREAMS streams
+  // forked after the uploads (ev_pf_fork) and joined before the iteration's
+  // counters are read, so one job's launch tail overlaps the next job's work
+  // and the class kernels
+  cudaStream_t st_pf[RB_PF_STREAMS] = {};
+  cudaEvent_t ev_pf_fork = nullptr, ev_pf_join[RB_PF_STREAMS] = {};
   // job buffers come from a private stream-ordered pool that keeps freed
   // memory (the device's default pool hands it back at every synchronisation,
   // and mapping it again on the next admission stalls the loop)
@@ -676,14 +684,24 @@ static int server_step(Server &S) {
   };
   const long long frame_blocks_cap = (S.o.paths_per_iteration + 255) / 256 + 1;
   auto run_per_frame = [&]() -> int {
-    for (size_t k : pf_k) {
+    int used = 0, rc = RB_OK;
+    for (size_t i = 0; i < pf_k.size() && rc == RB_OK; ++i) {
+      const size_t k = pf_k[i];
       const Job &J = S.jobs[plan[k].id];
       const BatchJob &B = S.h_jobs[k];
       const int n = J.req.width * J.req.height;
-      const int rc = launch_render(S.scenes[J.req.scene], B.G, B.P, J.acc, J.acc + n, nullptr, S.d_pfc, S.st);
-      if (rc != RB_OK) return rc;
+      cudaStream_t ps = S.st_pf[i % RB_PF_STREAMS];
+      if (i < RB_PF_STREAMS) {
+        cudaStreamWaitEvent(ps, S.ev_pf_fork, 0);
+        ++used;
+      }
+      rc = launch_render(S.scenes[J.req.scene], B.G, B.P, J.acc, J.acc + n, nullptr, S.d_pfc, ps);
     }
-    return RB_OK;
+    for (int q = 0; q < used; ++q) {  // join, also after an error
+      cudaEventRecord(S.ev_pf_join[q], S.st_pf[q]);
+      cudaStreamWaitEvent(S.st, S.ev_pf_join[q], 0);
+    }
+    return rc;
   };
   if (S.o.use_graph && wf_k.empty() && pf_k.empty() && !(frames && (tb + 255) / 256 > frame_blocks_cap)) {
     // One graph, reused every iteration: table and control blocks are copied
@@ -720,7 +738,10 @@ static int server_step(Server &S) {
     cudaMemcpyAsync(S.d_jobs, S.h_jobs, sizeof(BatchJob) * plan.size(), cudaMemcpyHostToDevice, S.st);
     cudaMemcpyAsync(S.d_ctl, S.h_ctl, sizeof(BatchCtl) * RB_GROUPS, cudaMemcpyHostToDevice, S.st);
     cudaEventRecord(S.ev_up, S.st);
-    if (!pf_k.empty()) cudaMemsetAsync(S.d_pfc, 0, sizeof(unsigned long long) * 4, S.st);
+    if (!pf_k.empty()) {
+      cudaMemsetAsync(S.d_pfc, 0, sizeof(unsigned long long) * 4, S.st);
+      cudaEventRecord(S.ev_pf_fork, S.st);
+    }
     kernels(false);
     if (!pf_k.empty()) {
       const int rc = run_per_frame();
@@ -912,9 +933,14 @@ rb_server *rb_server_create(const rb_server_opts *opts, void *stream) {
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(S.pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  if (!cuda_ok(cudaStreamCreateWithFlags(&S.st_wf, cudaStreamNonBlocking), "server wavefront stream") ||
-      !cuda_ok(cudaEventCreateWithFlags(&S.ev_up, cudaEventDisableTiming), "server event") ||
-      !cuda_ok(cudaEventCreateWithFlags(&S.ev_wf, cudaEventDisableTiming), "server event")) {
+  bool streams_ok = cuda_ok(cudaStreamCreateWithFlags(&S.st_wf, cudaStreamNonBlocking), "server wavefront stream") &&
+                    cuda_ok(cudaEventCreateWithFlags(&S.ev_up, cudaEventDisableTiming), "server event") &&
+                    cuda_ok(cudaEventCreateWithFlags(&S.ev_wf, cudaEventDisableTiming), "server event") &&
+                    cuda_ok(cudaEventCreateWithFlags(&S.ev_pf_fork, cudaEventDisableTiming), "server event");
+  for (int q = 0; q < RB_PF_STREAMS && streams_ok; ++q)
+    streams_ok = cuda_ok(cudaStreamCreateWithFlags(&S.st_pf[q], cudaStreamNonBlocking), "server per-frame stream") &&
+                 cuda_ok(cudaEventCreateWithFlags(&S.ev_pf_join[q], cudaEventDisableTiming), "server event");
+  if (!streams_ok) {
     rb_server_destroy(r);
     return nullptr;
   }
@@ -947,6 +973,14 @@ void rb_server_destroy(rb_server *r) {
   }
   if (S.ev_up) cudaEventDestroy(S.ev_up);
   if (S.ev_wf) cudaEventDestroy(S.ev_wf);
+  for (int q = 0; q < RB_PF_STREAMS; ++q) {
+    if (S.st_pf[q]) {
+      cudaStreamSynchronize(S.st_pf[q]);
+      cudaStreamDestroy(S.st_pf[q]);
+    }
+    if (S.ev_pf_join[q]) cudaEventDestroy(S.ev_pf_join[q]);
+  }
+  if (S.ev_pf_fork) cudaEventDestroy(S.ev_pf_fork);
   if (S.pool) {
     if (S.st) cudaStreamSynchronize(S.st);  // the jobs' stream-ordered frees have run
     cudaMemPoolDestroy(S.pool);
