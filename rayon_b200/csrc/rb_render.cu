@@ -406,6 +406,10 @@ UploadRing g_rings[64];  // one per device (events and buffers of that device's 
 
 // memcpy on up to eight host threads (more do not raise host memory bandwidth)
 void copy_parallel(char *dst, const char *src, size_t n) {
+  if (n < (1u << 20)) {  // below 1 MB a thread costs more than it copies
+    std::memcpy(dst, src, n);
+    return;
+  }
   const size_t threads = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 8);
   const size_t chunk = (n + threads - 1) / threads;
   std::vector<std::thread> pool;
