@@ -203,7 +203,20 @@ def roofline(workload, peaks, peaks_kind, sm_mhz, t_ms, kernel_ms, segs, npaths,
            "step time x the kernel's share of the step (ncu launch list)",
            "traffic": prof.get("dram_bytes_per_launch"), "hbm": hbm}
     inst = prof.get("inst_executed_per_launch")
-    if inst:
+    per_step = prof.get("inst_executed_per_step")
+    if not inst and per_step:
+        # an engine of many launches (the wavefront engine): every warp
+        # instruction of its kernels in one timed step over the step's device time
+        ks = t_ms * 1e-3
+        out["kernel_ms"] = t_ms
+        out["kernel_ms_source"] = "the timed step (all of the engine's launches)"
+        peak = SMS * SCHEDULERS * sm_mhz * 1e6 / 1e9
+        ach = per_step / ks / 1e9
+        out.update({"bound": "issue", "achieved": ach, "peak": peak, "unit": "Gwarp-inst/s", "frac": ach / peak,
+                    "peak_kind": f"148 SMs x 4 schedulers x 1 warp-instruction/clock at the sampled {sm_mhz:.0f} MHz",
+                    "inst_executed_per_step": per_step, "ncu_case": prof.get("ncu_case"),
+                    "kernel": prof.get("kernel", "wavefront engine")})
+    elif inst:
         peak = SMS * SCHEDULERS * sm_mhz * 1e6 / 1e9
         ach = inst / ks / 1e9
         out.update({"bound": "issue", "achieved": ach, "peak": peak, "unit": "Gwarp-inst/s", "frac": ach / peak,
@@ -460,6 +473,7 @@ def main():
                     help="jobs of the serving section's stream (2000 = the full specified stream, ~15 min)")
     ap.add_argument("--serving-by-scene", action="store_true",
                     help="serving section: also serve each scene's jobs alone (served/plain per scene)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the e2e repetitions (profiling runs)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case for ncu: same frame at 16 spp (two views at most), no e2e/baselines")
     args = ap.parse_args()
