@@ -204,6 +204,10 @@ def roofline(workload, peaks, peaks_kind, sm_mhz, t_ms, kernel_ms, segs, npaths,
            "traffic": prof.get("dram_bytes_per_launch"), "hbm": hbm}
     inst = prof.get("inst_executed_per_launch")
     per_step = prof.get("inst_executed_per_step")
+    if not per_step and prof.get("inst_executed_per_path"):
+        # warp instructions per path from a smaller capture of the same
+        # workload, times this step's paths (the count grows with the paths)
+        per_step = prof["inst_executed_per_path"] * npaths
     if not inst and per_step:
         # an engine of many launches (the wavefront engine): every warp
         # instruction of its kernels in one timed step over the step's device time
@@ -215,6 +219,7 @@ def roofline(workload, peaks, peaks_kind, sm_mhz, t_ms, kernel_ms, segs, npaths,
         out.update({"bound": "issue", "achieved": ach, "peak": peak, "unit": "Gwarp-inst/s", "frac": ach / peak,
                     "peak_kind": f"148 SMs x 4 schedulers x 1 warp-instruction/clock at the sampled {sm_mhz:.0f} MHz",
                     "inst_executed_per_step": per_step, "ncu_case": prof.get("ncu_case"),
+                    "inst_executed_per_path": prof.get("inst_executed_per_path"),
                     "kernel": prof.get("kernel", "wavefront engine")})
     elif inst:
         peak = SMS * SCHEDULERS * sm_mhz * 1e6 / 1e9
