@@ -74,6 +74,72 @@ struct WfParams {
   int cap;
 };
 
+// Claims of the engine's shared counters (queue fill, march list, work
+// items). All of them are one address each, and the L2 serialises atomics on
+// one address: one atomic per warp in a launch of 16 M slots is 512 K atomics
+// on each counter. With WF_BLOCK_CLAIM a block claims for all its warps at
+// once (one atomic per 256 threads).
+#ifndef WF_BLOCK_CLAIM
+#define WF_BLOCK_CLAIM 1
+#endif
+// List entries a march warp claims at once when it runs short (0: one claim
+// per refill of exactly the lanes that need a ray).
+#ifndef WF_MARCH_CHUNK
+#define WF_MARCH_CHUNK 32
+#endif
+
+// Every thread of the block calls it (it synchronises the block three times).
+// Threads with `want` receive consecutive indices, in warp then lane order,
+// from one atomicAdd of the block's total on *counter; the others get
+// (T)-1. *total receives the block's total.
+template <typename T>
+__device__ __forceinline__ T block_claim(T *counter, bool want, T &total) {
+  __shared__ unsigned s_warp[33];
+  __shared__ T s_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (lane == 0) s_warp[warp] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      const unsigned c = s_warp[w];
+      s_warp[w] = tot;
+      tot += c;
+    }
+    s_warp[32] = tot;
+    s_base = tot ? atomicAdd(counter, (T)tot) : (T)0;
+  }
+  __syncthreads();
+  total = (T)s_warp[32];
+  const T idx = want ? s_base + (T)s_warp[warp] + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
+  __syncthreads();  // the shared words are free for the next claim
+  return idx;
+}
+
+// One warp's claim (the leader's atomic, broadcast).
+template <typename T>
+__device__ __forceinline__ T warp_claim(T *counter, bool want, T &total) {
+  const int lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  total = (T)__popc(m);
+  if (!m) return (T)-1;
+  T base = 0;
+  const int leader = __ffs(m) - 1;
+  if (lane == leader) base = atomicAdd(counter, total);
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return want ? base + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
+}
+
+template <typename T>
+__device__ __forceinline__ T wf_claim(T *counter, bool want, T &total) {
+#if WF_BLOCK_CLAIM
+  return block_claim<T>(counter, want, total);
+#else
+  return warp_claim<T>(counter, want, total);
+#endif
+}
+
 __device__ __forceinline__ bool wf_marches(const WfParams &W) {
   return W.cand != nullptr && W.S.sdf_k > 0.0f && W.S.num_sdf > 0;
 }
@@ -182,15 +248,10 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
   if (MS >= RB_MS_SDF) {
-    // append the warp's marching rays to the list (one atomic per warp)
-    const unsigned mask = __ballot_sync(0xffffffffu, march);
-    if (mask) {
-      int base = 0;
-      const int leader = __ffs(mask) - 1;
-      if (lane == leader) base = atomicAdd(&W.ctl->march_count, __popc(mask));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (march) W.list[base + __popc(mask & ((1u << lane) - 1u))] = k;
-    }
+    // append the marching rays to the list
+    int n_march = 0;
+    const int at = wf_claim<int>(&W.ctl->march_count, march, n_march);
+    if (march) W.list[at] = k;
   }
 }
 
@@ -413,16 +474,38 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
   r.o = r.d = f3(0.f, 0.f, 0.f);
   bool busy = false, drained = false;
   unsigned long long passes = 0;
+  unsigned cl_next = 0, cl_end = 0;  // the warp's claimed list range (the same in every lane)
   while (true) {
     const bool need = !busy && !drained;
     const unsigned mask = __ballot_sync(0xffffffffu, need);
     if (mask) {
-      unsigned base = 0;
       const int leader = __ffs(mask) - 1;
-      if (lane == leader) base = atomicAdd(&W.ctl->march_next, (unsigned)__popc(mask));
-      base = __shfl_sync(0xffffffffu, base, leader);
+      const unsigned want = (unsigned)__popc(mask), rank = (unsigned)__popc(mask & ((1u << lane) - 1u));
+      unsigned idx_base = 0;  // this lane's list entry is idx_base + rank (below) or in the new range
+#if WF_MARCH_CHUNK
+      // the warp keeps a claimed range [cl_next, cl_end) of list entries and
+      // takes a new range of at least WF_MARCH_CHUNK when it runs short (one
+      // atomic per range instead of one per refill)
+      const unsigned avail = cl_end - cl_next;
+      unsigned nb = 0, take = 0;
+      if (avail < want) {
+        take = want - avail > WF_MARCH_CHUNK ? want - avail : WF_MARCH_CHUNK;
+        if (lane == leader) nb = atomicAdd(&W.ctl->march_next, take);
+        nb = __shfl_sync(0xffffffffu, nb, leader);
+      }
+      idx_base = rank < avail ? cl_next : nb - avail;
+      if (avail >= want) {
+        cl_next += want;
+      } else {
+        cl_next = nb + (want - avail);
+        cl_end = nb + take;
+      }
+#else
+      if (lane == leader) idx_base = atomicAdd(&W.ctl->march_next, want);
+      idx_base = __shfl_sync(0xffffffffu, idx_base, leader);
+#endif
       if (need) {
-        const unsigned idx = base + __popc(mask & ((1u << lane) - 1u));
+        const unsigned idx = idx_base + rank;
         if (idx < total) {
           slot = W.list[idx];
           if constexpr (MASK) {
@@ -663,43 +746,42 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
     }
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
-  // regeneration: ended paths claim the next work items (one atomic per warp)
-  const unsigned rmask = __ballot_sync(0xffffffffu, regenerate);
-  unsigned long long item = ~0ull;
-  if (rmask) {
-    unsigned long long base = 0;
-    const int leader = __ffs(rmask) - 1;
-    if (lane == leader) base = atomicAdd(&W.ctl->next_path, (unsigned long long)__popc(rmask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (regenerate) {
-      item = base + __popc(rmask & ((1u << lane) - 1u));
-      if (item >= W.ctl->total_paths) item = ~0ull;
-    }
-    if (lane == leader) atomicAdd(&W.ctl->paths_done, (unsigned long long)__popc(rmask));
-  }
+  // regeneration: ended paths claim the next work items
+  unsigned long long ended_paths = 0;
+  unsigned long long item = wf_claim<unsigned long long>(&W.ctl->next_path, regenerate, ended_paths);
+  if (regenerate && item >= W.ctl->total_paths) item = ~0ull;
+  if (ended_paths && (WF_BLOCK_CLAIM ? threadIdx.x == 0 : lane == __ffs(__activemask()) - 1))
+    atomicAdd(&W.ctl->paths_done, ended_paths);
   const bool emits = have_out || item != ~0ull;
-  // compaction into the output queue (one atomic per warp)
-  const unsigned omask = __ballot_sync(0xffffffffu, emits);
-  if (omask) {
-    int base = 0;
-    const int leader = __ffs(omask) - 1;
-    if (lane == leader) base = atomicAdd(&W.ctl->count[qi ^ 1], __popc(omask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    const int slot = base + __popc(omask & ((1u << lane) - 1u));
-    if (have_out) {
-      out.o[slot] = no;
-      out.d[slot] = nd;
-      out.thr[slot] = nthr;
-      out.L[slot] = nL;
-      out.meta[slot] = nmeta;
-    } else if (emits) {
-      wf_emit_camera(W, out, slot, item);
-    }
+  // compaction into the output queue
+  int n_emit = 0;
+  const int slot = wf_claim<int>(&W.ctl->count[qi ^ 1], emits, n_emit);
+  if (have_out) {
+    out.o[slot] = no;
+    out.d[slot] = nd;
+    out.thr[slot] = nthr;
+    out.L[slot] = nL;
+    out.meta[slot] = nmeta;
+  } else if (emits) {
+    wf_emit_camera(W, out, slot, item);
   }
-  const unsigned long long segs = (k < n_in) ? 1ull : 0ull;
-  unsigned long long s = segs;
-  for (int o2 = 16; o2 > 0; o2 >>= 1) s += __shfl_down_sync(0xffffffffu, s, o2);
-  if (lane == 0 && s) atomicAdd(&W.ctl->segments, s);
+  // segments: one count per live input slot (one atomic per block or warp)
+  const int live = k < n_in ? 1 : 0;
+  unsigned long long n_live = 0;
+#if WF_BLOCK_CLAIM
+  {
+    __shared__ unsigned s_live;
+    if (threadIdx.x == 0) s_live = 0;
+    __syncthreads();
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    if (lane == 0 && m) atomicAdd(&s_live, (unsigned)__popc(m));
+    __syncthreads();
+    n_live = threadIdx.x == 0 ? s_live : 0;
+  }
+#else
+  n_live = lane == 0 ? (unsigned long long)__popc(__ballot_sync(0xffffffffu, live)) : 0;
+#endif
+  if (n_live) atomicAdd(&W.ctl->segments, n_live);
 }
 
 // Resets the live count of the queue the next shade writes into, and the march list.
