@@ -625,6 +625,11 @@ __global__ void __launch_bounds__(256, WF_MARCH_MINB) k_wf_march(WfParams W, WfQ
   if (lane == 0 && passes) atomicAdd(&W.ctl->march_steps, passes);
 }
 
+// Threads per shade block (a block claims once for all its warps, so its
+// warps wait for one another at the claim).
+#ifndef WF_SHADE_THREADS
+#define WF_SHADE_THREADS 256
+#endif
 #ifndef WF_SHADE_MINB
 #define WF_SHADE_MINB 2
 #endif
@@ -746,16 +751,68 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
     }
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
-  // regeneration: ended paths claim the next work items
+#if WF_BLOCK_CLAIM
+  // One pass over the block, two barriers: per warp the regenerating, the
+  // surviving and the live lanes; one thread claims the block's work items
+  // and, knowing how many of them exist, its output slots (survivors first,
+  // then the new paths), and adds the block's counts.
+  __shared__ unsigned s_cnt[3][32];
+  __shared__ unsigned long long s_item;
+  __shared__ int s_slot;
+  __shared__ unsigned s_valid, s_out;
+  const int warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned mr = __ballot_sync(0xffffffffu, regenerate), mo = __ballot_sync(0xffffffffu, have_out);
+  const unsigned ml = __ballot_sync(0xffffffffu, k < n_in);
+  if (lane == 0) {
+    s_cnt[0][warp] = __popc(mr);
+    s_cnt[1][warp] = __popc(mo);
+    s_cnt[2][warp] = __popc(ml);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned R = 0, O = 0, live = 0;
+    for (int w = 0; w < nw; ++w) {
+      const unsigned r = s_cnt[0][w], o = s_cnt[1][w];
+      s_cnt[0][w] = R;
+      s_cnt[1][w] = O;
+      R += r;
+      O += o;
+      live += s_cnt[2][w];
+    }
+    const unsigned long long base = R ? atomicAdd(&W.ctl->next_path, (unsigned long long)R) : 0ull;
+    const unsigned long long total = W.ctl->total_paths;
+    const unsigned valid = base >= total ? 0u : (unsigned)(total - base < R ? total - base : R);
+    s_item = base;
+    s_valid = valid;
+    s_out = O;
+    s_slot = (O + valid) ? atomicAdd(&W.ctl->count[qi ^ 1], (int)(O + valid)) : 0;
+    if (R) atomicAdd(&W.ctl->paths_done, (unsigned long long)R);
+    if (live) atomicAdd(&W.ctl->segments, (unsigned long long)live);
+  }
+  __syncthreads();
+  if (have_out) {
+    const int slot = s_slot + (int)(s_cnt[1][warp] + __popc(mo & lt));
+    out.o[slot] = no;
+    out.d[slot] = nd;
+    out.thr[slot] = nthr;
+    out.L[slot] = nL;
+    out.meta[slot] = nmeta;
+  } else if (regenerate) {
+    const unsigned r = s_cnt[0][warp] + __popc(mr & lt);
+    if (r < s_valid) wf_emit_camera(W, out, s_slot + (int)(s_out + r), s_item + r);
+  }
+}
+#else
+  // regeneration: ended paths claim the next work items (one atomic per warp)
   unsigned long long ended_paths = 0;
-  unsigned long long item = wf_claim<unsigned long long>(&W.ctl->next_path, regenerate, ended_paths);
+  unsigned long long item = warp_claim<unsigned long long>(&W.ctl->next_path, regenerate, ended_paths);
   if (regenerate && item >= W.ctl->total_paths) item = ~0ull;
-  if (ended_paths && (WF_BLOCK_CLAIM ? threadIdx.x == 0 : lane == __ffs(__activemask()) - 1))
-    atomicAdd(&W.ctl->paths_done, ended_paths);
+  if (ended_paths && lane == __ffs(__activemask()) - 1) atomicAdd(&W.ctl->paths_done, ended_paths);
   const bool emits = have_out || item != ~0ull;
-  // compaction into the output queue
+  // compaction into the output queue (one atomic per warp)
   int n_emit = 0;
-  const int slot = wf_claim<int>(&W.ctl->count[qi ^ 1], emits, n_emit);
+  const int slot = warp_claim<int>(&W.ctl->count[qi ^ 1], emits, n_emit);
   if (have_out) {
     out.o[slot] = no;
     out.d[slot] = nd;
@@ -765,24 +822,10 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
   } else if (emits) {
     wf_emit_camera(W, out, slot, item);
   }
-  // segments: one count per live input slot (one atomic per block or warp)
-  const int live = k < n_in ? 1 : 0;
-  unsigned long long n_live = 0;
-#if WF_BLOCK_CLAIM
-  {
-    __shared__ unsigned s_live;
-    if (threadIdx.x == 0) s_live = 0;
-    __syncthreads();
-    const unsigned m = __ballot_sync(0xffffffffu, live);
-    if (lane == 0 && m) atomicAdd(&s_live, (unsigned)__popc(m));
-    __syncthreads();
-    n_live = threadIdx.x == 0 ? s_live : 0;
-  }
-#else
-  n_live = lane == 0 ? (unsigned long long)__popc(__ballot_sync(0xffffffffu, live)) : 0;
-#endif
-  if (n_live) atomicAdd(&W.ctl->segments, n_live);
+  const unsigned ml = __ballot_sync(0xffffffffu, k < n_in);
+  if (lane == 0 && ml) atomicAdd(&W.ctl->segments, (unsigned long long)__popc(ml));
 }
+#endif
 
 // Resets the live count of the queue the next shade writes into, and the march list.
 __global__ void k_wf_reset(WfCtl *ctl, int qi) {
@@ -899,7 +942,9 @@ static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int m
     if (mask) k_wf_march<MS, true><<<march_grid, 256, tab, st>>>(W, E.q[qi], 1);
     else k_wf_march<MS, false><<<march_grid, 256, tab, st>>>(W, E.q[qi], tab > 0 ? 1 : 0);
   }
-  k_wf_shade<MS, NEE><<<grid, 256, sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
+  const int shade_grid = (E.capacity + WF_SHADE_THREADS - 1) / WF_SHADE_THREADS;
+  const size_t shade_sm = stack_smem_bytes(W.S.short_stack, WF_SHADE_THREADS);
+  k_wf_shade<MS, NEE><<<shade_grid, WF_SHADE_THREADS, shade_sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
 }
 
 template <int MS, bool NEE>
