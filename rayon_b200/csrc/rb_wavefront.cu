@@ -88,11 +88,12 @@ struct WfParams {
 #define WF_MARCH_CHUNK 32
 #endif
 
-// Every thread of the block calls it (it synchronises the block three times).
+// Every thread of the block calls it (it synchronises the block twice, and a
+// third time when kReuse: before the shared words serve another claim).
 // Threads with `want` receive consecutive indices, in warp then lane order,
 // from one atomicAdd of the block's total on *counter; the others get
 // (T)-1. *total receives the block's total.
-template <typename T>
+template <typename T, bool kReuse = true>
 __device__ __forceinline__ T block_claim(T *counter, bool want, T &total) {
   __shared__ unsigned s_warp[33];
   __shared__ T s_base;
@@ -113,7 +114,7 @@ __device__ __forceinline__ T block_claim(T *counter, bool want, T &total) {
   __syncthreads();
   total = (T)s_warp[32];
   const T idx = want ? s_base + (T)s_warp[warp] + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
-  __syncthreads();  // the shared words are free for the next claim
+  if (kReuse) __syncthreads();  // the shared words are free for the next claim
   return idx;
 }
 
@@ -131,10 +132,10 @@ __device__ __forceinline__ T warp_claim(T *counter, bool want, T &total) {
   return want ? base + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
 }
 
-template <typename T>
+template <typename T, bool kReuse = true>
 __device__ __forceinline__ T wf_claim(T *counter, bool want, T &total) {
 #if WF_BLOCK_CLAIM
-  return block_claim<T>(counter, want, total);
+  return block_claim<T, kReuse>(counter, want, total);
 #else
   return warp_claim<T>(counter, want, total);
 #endif
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
   if (MS >= RB_MS_SDF) {
     // append the marching rays to the list
     int n_march = 0;
-    const int at = wf_claim<int>(&W.ctl->march_count, march, n_march);
+    const int at = wf_claim<int, false>(&W.ctl->march_count, march, n_march);  // the block's last claim
     if (march) W.list[at] = k;
   }
 }
