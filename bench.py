@@ -474,10 +474,11 @@ def main():
     ap.add_argument("--workload", default="cornell", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the equal-RMSE and serving sections")
-    ap.add_argument("--serving-jobs", type=int, default=400,
-                    help="jobs of the serving section's stream (2000 = the full specified stream, ~15 min)")
-    ap.add_argument("--serving-by-scene", action="store_true",
-                    help="serving section: also serve each scene's jobs alone (served/plain per scene)")
+    ap.add_argument("--serving-jobs", type=int, default=2000,
+                    help="jobs of the serving section's stream (default: the full specified stream of 2000 "
+                         "Poisson arrivals at 50/s; about 9 minutes of plain and served runs)")
+    ap.add_argument("--serving-by-scene", type=int, nargs="?", const=1, default=1,
+                    help="serving section: also serve each scene's jobs alone (served/plain per scene; 0 = off)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the e2e repetitions (profiling runs)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case for ncu: same frame at 16 spp (two views at most), no e2e/baselines")
@@ -814,7 +815,7 @@ def reference_cuda(spec):
                     "e2e excludes its scene build and upload (scene_build_upload_s)"}
 
 
-def serving_section(n_jobs: int = 400, rate: float = 50.0, backlog: bool = False, by_scene: bool = False):
+def serving_section(n_jobs: int = 2000, rate: float = 50.0, backlog: bool = False, by_scene: bool = True):
     """The serving mix: n_jobs Poisson arrivals at `rate` jobs/s (2000 in the
     specified stream) over the One-Weekend, Cornell, icosphere and SDF scenes,
     resolutions from {256^2, 512^2, 1280x720, 1920x1080}, spp log-uniform
