@@ -82,6 +82,11 @@ struct WfParams {
 #ifndef WF_BLOCK_CLAIM
 #define WF_BLOCK_CLAIM 1
 #endif
+// The extend kernel's march-list appends: the block's last warp to finish
+// claims for the block (1), or every warp waits at a block claim (0).
+#ifndef WF_EXTEND_LAST
+#define WF_EXTEND_LAST 1
+#endif
 // List entries a march warp claims at once when it runs short (0: one claim
 // per refill of exactly the lanes that need a ray).
 #ifndef WF_MARCH_CHUNK
@@ -204,6 +209,17 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+#if WF_EXTEND_LAST
+  __shared__ int s_marched[256];      // the block's marching slots (blocks of at most 256 threads)
+  __shared__ unsigned s_nm, s_done;  // staged slots, finished warps
+  if (MS >= RB_MS_SDF) {
+    if (threadIdx.x == 0) {
+      s_nm = 0u;
+      s_done = 0u;
+    }
+    __syncthreads();  // at the start every warp arrives together
+  }
+#endif
   const bool valid = k < W.ctl->count[qi];
   bool march = false;
   if (valid) {
@@ -249,10 +265,37 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
   if (MS >= RB_MS_SDF) {
+#if WF_EXTEND_LAST
+    // append the marching rays to the list: each warp stages its slots in
+    // shared memory and leaves; the block's last warp to finish claims the
+    // block's range with one atomic and copies the slots out (no warp waits
+    // for the others)
+    const unsigned m = __ballot_sync(0xffffffffu, march);
+    if (m) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(&s_nm, (unsigned)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (march) s_marched[base + __popc(m & ((1u << lane) - 1u))] = k;
+    }
+    __syncwarp();
+    __threadfence_block();  // the staged slots before the finish count
+    unsigned done = 0;
+    if (lane == 0) done = atomicAdd(&s_done, 1u);
+    done = __shfl_sync(0xffffffffu, done, 0);
+    if (done == ((blockDim.x + 31u) >> 5) - 1u) {  // the last warp of the block
+      __threadfence_block();
+      const unsigned n = *static_cast<volatile unsigned *>(&s_nm);
+      int at = 0;
+      if (lane == 0 && n) at = atomicAdd(&W.ctl->march_count, (int)n);
+      at = __shfl_sync(0xffffffffu, at, 0);
+      for (unsigned i = lane; i < n; i += 32) W.list[at + (int)i] = static_cast<volatile int *>(s_marched)[i];
+    }
+#else
     // append the marching rays to the list
     int n_march = 0;
     const int at = wf_claim<int, false>(&W.ctl->march_count, march, n_march);  // the block's last claim
     if (march) W.list[at] = k;
+#endif
   }
 }
 
