@@ -59,6 +59,9 @@ struct WfCtl {
   int march_count;                // rays appended to the march list this iteration
   unsigned int march_next;        // next march-list entry to take
   unsigned long long march_steps;
+  unsigned long long regen_item;  // k_wf_regen: the first new work item,
+  int regen_slot;                 // its slot,
+  int regen_n;                    // and how many
 };
 
 struct WfParams {
@@ -74,76 +77,35 @@ struct WfParams {
   int cap;
 };
 
-// Claims of the engine's shared counters (queue fill, march list, work
-// items). All of them are one address each, and the L2 serialises atomics on
-// one address: one atomic per warp in a launch of 16 M slots is 512 K atomics
-// on each counter. With WF_BLOCK_CLAIM a block claims for all its warps at
-// once (one atomic per 256 threads).
-#ifndef WF_BLOCK_CLAIM
-#define WF_BLOCK_CLAIM 1
-#endif
-// The extend kernel's march-list appends: the block's last warp to finish
-// claims for the block (1), or every warp waits at a block claim (0).
-#ifndef WF_EXTEND_LAST
-#define WF_EXTEND_LAST 1
-#endif
+// The engine's shared counters (queue fill, march list, work items, segment
+// and path counts) are one address each, and the L2 serialises atomics on one
+// address: one atomic per warp in a launch of 16 M slots is 512 K atomics on
+// each. The extend and shade kernels therefore claim once per block, by the
+// block's last warp to finish: each warp stages what it produced in shared
+// memory and leaves, and a shared count of finished warps (after a block
+// fence) tells the last one, which claims the block's range with one atomic
+// and copies the staged entries out. No warp waits at a barrier for the
+// others. New camera paths are not emitted by the shade kernel: a separate
+// launch fills the output queue's free slots with consecutive work items
+// (k_wf_regen_plan, k_wf_regen).
+
 // List entries a march warp claims at once when it runs short (0: one claim
 // per refill of exactly the lanes that need a ray).
 #ifndef WF_MARCH_CHUNK
 #define WF_MARCH_CHUNK 32
 #endif
 
-// Every thread of the block calls it (it synchronises the block twice, and a
-// third time when kReuse: before the shared words serve another claim).
-// Threads with `want` receive consecutive indices, in warp then lane order,
-// from one atomicAdd of the block's total on *counter; the others get
-// (T)-1. *total receives the block's total.
-template <typename T, bool kReuse = true>
-__device__ __forceinline__ T block_claim(T *counter, bool want, T &total) {
-  __shared__ unsigned s_warp[33];
-  __shared__ T s_base;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  const unsigned m = __ballot_sync(0xffffffffu, want);
-  if (lane == 0) s_warp[warp] = __popc(m);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned tot = 0;
-    for (int w = 0; w < nw; ++w) {
-      const unsigned c = s_warp[w];
-      s_warp[w] = tot;
-      tot += c;
-    }
-    s_warp[32] = tot;
-    s_base = tot ? atomicAdd(counter, (T)tot) : (T)0;
-  }
-  __syncthreads();
-  total = (T)s_warp[32];
-  const T idx = want ? s_base + (T)s_warp[warp] + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
-  if (kReuse) __syncthreads();  // the shared words are free for the next claim
-  return idx;
-}
-
-// One warp's claim (the leader's atomic, broadcast).
-template <typename T>
-__device__ __forceinline__ T warp_claim(T *counter, bool want, T &total) {
-  const int lane = threadIdx.x & 31;
-  const unsigned m = __ballot_sync(0xffffffffu, want);
-  total = (T)__popc(m);
-  if (!m) return (T)-1;
-  T base = 0;
-  const int leader = __ffs(m) - 1;
-  if (lane == leader) base = atomicAdd(counter, total);
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return want ? base + (T)__popc(m & ((1u << lane) - 1u)) : (T)-1;
-}
-
-template <typename T, bool kReuse = true>
-__device__ __forceinline__ T wf_claim(T *counter, bool want, T &total) {
-#if WF_BLOCK_CLAIM
-  return block_claim<T, kReuse>(counter, want, total);
-#else
-  return warp_claim<T>(counter, want, total);
-#endif
+// True for the block's last warp to arrive (call once per warp, after the
+// warp's shared-memory writes; `done` is a zeroed shared counter).
+__device__ __forceinline__ bool wf_last_warp(unsigned *done) {
+  __syncwarp();
+  __threadfence_block();
+  unsigned d = 0;
+  if ((threadIdx.x & 31) == 0) d = atomicAdd(done, 1u);
+  d = __shfl_sync(0xffffffffu, d, 0);
+  const bool last = d == ((blockDim.x + 31u) >> 5) - 1u;
+  if (last) __threadfence_block();
+  return last;
 }
 
 __device__ __forceinline__ bool wf_marches(const WfParams &W) {
@@ -209,7 +171,6 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
   extern __shared__ int2 smem[];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-#if WF_EXTEND_LAST
   __shared__ int s_marched[256];      // the block's marching slots (blocks of at most 256 threads)
   __shared__ unsigned s_nm, s_done;  // staged slots, finished warps
   if (MS >= RB_MS_SDF) {
@@ -219,7 +180,6 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
     }
     __syncthreads();  // at the start every warp arrives together
   }
-#endif
   const bool valid = k < W.ctl->count[qi];
   bool march = false;
   if (valid) {
@@ -265,7 +225,6 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
   if (MS >= RB_MS_SDF) {
-#if WF_EXTEND_LAST
     // append the marching rays to the list: each warp stages its slots in
     // shared memory and leaves; the block's last warp to finish claims the
     // block's range with one atomic and copies the slots out (no warp waits
@@ -277,25 +236,13 @@ __global__ void __launch_bounds__(256, WF_EXTEND_MINB) k_wf_extend(const RB_GRID
       base = __shfl_sync(0xffffffffu, base, 0);
       if (march) s_marched[base + __popc(m & ((1u << lane) - 1u))] = k;
     }
-    __syncwarp();
-    __threadfence_block();  // the staged slots before the finish count
-    unsigned done = 0;
-    if (lane == 0) done = atomicAdd(&s_done, 1u);
-    done = __shfl_sync(0xffffffffu, done, 0);
-    if (done == ((blockDim.x + 31u) >> 5) - 1u) {  // the last warp of the block
-      __threadfence_block();
+    if (wf_last_warp(&s_done)) {
       const unsigned n = *static_cast<volatile unsigned *>(&s_nm);
       int at = 0;
       if (lane == 0 && n) at = atomicAdd(&W.ctl->march_count, (int)n);
       at = __shfl_sync(0xffffffffu, at, 0);
       for (unsigned i = lane; i < n; i += 32) W.list[at + (int)i] = static_cast<volatile int *>(s_marched)[i];
     }
-#else
-    // append the marching rays to the list
-    int n_march = 0;
-    const int at = wf_claim<int, false>(&W.ctl->march_count, march, n_march);  // the block's last claim
-    if (march) W.list[at] = k;
-#endif
   }
 }
 
@@ -683,6 +630,15 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int n_in = W.ctl->count[qi];
+  __shared__ float4 s_rec[5 * WF_SHADE_THREADS];  // the block's surviving paths (o, d, thr, L, meta)
+  __shared__ unsigned s_nout, s_nend, s_nlive, s_done;
+  if (threadIdx.x == 0) {
+    s_nout = 0u;
+    s_nend = 0u;
+    s_nlive = 0u;
+    s_done = 0u;
+  }
+  __syncthreads();  // at the start every warp arrives together
   bool have_out = false;
   // outgoing path, held in registers until the warp's range is reserved
   float4 no = make_float4(0, 0, 0, 0), nd = no, nthr = no, nL = no;
@@ -795,83 +751,78 @@ __global__ void __launch_bounds__(256, WF_SHADE_MINB) k_wf_shade(WfParams W, WfQ
     }
     if (ovf) atomicAdd(&W.ctl->overflow, (unsigned long long)ovf);
   }
-#if WF_BLOCK_CLAIM
-  // One pass over the block, two barriers: per warp the regenerating, the
-  // surviving and the live lanes; one thread claims the block's work items
-  // and, knowing how many of them exist, its output slots (survivors first,
-  // then the new paths), and adds the block's counts.
-  __shared__ unsigned s_cnt[3][32];
-  __shared__ unsigned long long s_item;
-  __shared__ int s_slot;
-  __shared__ unsigned s_valid, s_out;
-  const int warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  const unsigned mr = __ballot_sync(0xffffffffu, regenerate), mo = __ballot_sync(0xffffffffu, have_out);
+  // Survivors are compacted into the output queue by the block's last warp
+  // (each warp stages its surviving paths in shared memory and leaves); the
+  // ended paths are only counted: k_wf_regen fills the free slots with new
+  // camera paths after this launch.
+  const unsigned mo = __ballot_sync(0xffffffffu, have_out), me = __ballot_sync(0xffffffffu, regenerate);
   const unsigned ml = __ballot_sync(0xffffffffu, k < n_in);
+  unsigned off = 0;
   if (lane == 0) {
-    s_cnt[0][warp] = __popc(mr);
-    s_cnt[1][warp] = __popc(mo);
-    s_cnt[2][warp] = __popc(ml);
+    if (mo) off = atomicAdd(&s_nout, (unsigned)__popc(mo));
+    if (me) atomicAdd(&s_nend, (unsigned)__popc(me));
+    if (ml) atomicAdd(&s_nlive, (unsigned)__popc(ml));
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned R = 0, O = 0, live = 0;
-    for (int w = 0; w < nw; ++w) {
-      const unsigned r = s_cnt[0][w], o = s_cnt[1][w];
-      s_cnt[0][w] = R;
-      s_cnt[1][w] = O;
-      R += r;
-      O += o;
-      live += s_cnt[2][w];
+  off = __shfl_sync(0xffffffffu, off, 0);
+  if (have_out) {
+    float4 *rec = s_rec + 5 * (off + __popc(mo & ((1u << lane) - 1u)));
+    rec[0] = no;
+    rec[1] = nd;
+    rec[2] = nthr;
+    rec[3] = nL;
+    rec[4] = make_float4(__int_as_float(nmeta.x), __int_as_float(nmeta.y), __int_as_float(nmeta.z),
+                         __int_as_float(nmeta.w));
+  }
+  if (wf_last_warp(&s_done)) {
+    const unsigned n_out = *static_cast<volatile unsigned *>(&s_nout);
+    int at = 0;
+    if (lane == 0) {
+      if (n_out) at = atomicAdd(&W.ctl->count[qi ^ 1], (int)n_out);
+      const unsigned n_end = *static_cast<volatile unsigned *>(&s_nend);
+      const unsigned n_live = *static_cast<volatile unsigned *>(&s_nlive);
+      if (n_end) atomicAdd(&W.ctl->paths_done, (unsigned long long)n_end);
+      if (n_live) atomicAdd(&W.ctl->segments, (unsigned long long)n_live);
     }
-    const unsigned long long base = R ? atomicAdd(&W.ctl->next_path, (unsigned long long)R) : 0ull;
-    const unsigned long long total = W.ctl->total_paths;
-    const unsigned valid = base >= total ? 0u : (unsigned)(total - base < R ? total - base : R);
-    s_item = base;
-    s_valid = valid;
-    s_out = O;
-    s_slot = (O + valid) ? atomicAdd(&W.ctl->count[qi ^ 1], (int)(O + valid)) : 0;
-    if (R) atomicAdd(&W.ctl->paths_done, (unsigned long long)R);
-    if (live) atomicAdd(&W.ctl->segments, (unsigned long long)live);
-  }
-  __syncthreads();
-  if (have_out) {
-    const int slot = s_slot + (int)(s_cnt[1][warp] + __popc(mo & lt));
-    out.o[slot] = no;
-    out.d[slot] = nd;
-    out.thr[slot] = nthr;
-    out.L[slot] = nL;
-    out.meta[slot] = nmeta;
-  } else if (regenerate) {
-    const unsigned r = s_cnt[0][warp] + __popc(mr & lt);
-    if (r < s_valid) wf_emit_camera(W, out, s_slot + (int)(s_out + r), s_item + r);
+    at = __shfl_sync(0xffffffffu, at, 0);
+    const volatile float4 *vr = s_rec;
+    for (unsigned i = lane; i < n_out; i += 32) {
+      const volatile float4 *rec = vr + 5 * i;
+      const int slot = at + (int)i;
+      out.o[slot] = make_float4(rec[0].x, rec[0].y, rec[0].z, rec[0].w);
+      out.d[slot] = make_float4(rec[1].x, rec[1].y, rec[1].z, rec[1].w);
+      out.thr[slot] = make_float4(rec[2].x, rec[2].y, rec[2].z, rec[2].w);
+      out.L[slot] = make_float4(rec[3].x, rec[3].y, rec[3].z, rec[3].w);
+      out.meta[slot] = make_int4(__float_as_int(rec[4].x), __float_as_int(rec[4].y), __float_as_int(rec[4].z),
+                                 __float_as_int(rec[4].w));
+    }
   }
 }
-#else
-  // regeneration: ended paths claim the next work items (one atomic per warp)
-  unsigned long long ended_paths = 0;
-  unsigned long long item = warp_claim<unsigned long long>(&W.ctl->next_path, regenerate, ended_paths);
-  if (regenerate && item >= W.ctl->total_paths) item = ~0ull;
-  if (ended_paths && lane == __ffs(__activemask()) - 1) atomicAdd(&W.ctl->paths_done, ended_paths);
-  const bool emits = have_out || item != ~0ull;
-  // compaction into the output queue (one atomic per warp)
-  int n_emit = 0;
-  const int slot = warp_claim<int>(&W.ctl->count[qi ^ 1], emits, n_emit);
-  if (have_out) {
-    out.o[slot] = no;
-    out.d[slot] = nd;
-    out.thr[slot] = nthr;
-    out.L[slot] = nL;
-    out.meta[slot] = nmeta;
-  } else if (emits) {
-    wf_emit_camera(W, out, slot, item);
-  }
-  const unsigned ml = __ballot_sync(0xffffffffu, k < n_in);
-  if (lane == 0 && ml) atomicAdd(&W.ctl->segments, (unsigned long long)__popc(ml));
-}
-#endif
 
 // Resets the live count of the queue the next shade writes into, and the march list.
+// After a shade launch into queue qo: the free slots of queue qo (from the
+// survivors' count to the capacity) take the next work items, as many as
+// remain (one thread).
+__global__ void k_wf_regen_plan(WfCtl *ctl, int qo, int capacity) {
+  const int S = ctl->count[qo];
+  const unsigned long long P = ctl->next_path, T = ctl->total_paths;
+  const unsigned long long room = (unsigned long long)(capacity > S ? capacity - S : 0);
+  const unsigned long long n = P < T ? (T - P < room ? T - P : room) : 0ull;
+  ctl->regen_item = P;
+  ctl->regen_slot = S;
+  ctl->regen_n = (int)n;
+  ctl->next_path = P + n;
+  ctl->count[qo] = S + (int)n;
+}
+
+// New camera paths into the planned slots: slot regen_slot + t takes work
+// item regen_item + t (consecutive items: neighbouring pixels of one sample,
+// so a warp's camera rays start together).
+__global__ void k_wf_regen(const RB_GRID_CONST WfParams W, const RB_GRID_CONST WfQueue q) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= W.ctl->regen_n) return;
+  wf_emit_camera(W, q, W.ctl->regen_slot + t, W.ctl->regen_item + (unsigned long long)t);
+}
+
 __global__ void k_wf_reset(WfCtl *ctl, int qi) {
   ctl->count[qi] = 0;
   ctl->march_count = 0;
@@ -989,6 +940,8 @@ static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int m
   const int shade_grid = (E.capacity + WF_SHADE_THREADS - 1) / WF_SHADE_THREADS;
   const size_t shade_sm = stack_smem_bytes(W.S.short_stack, WF_SHADE_THREADS);
   k_wf_shade<MS, NEE><<<shade_grid, WF_SHADE_THREADS, shade_sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
+  k_wf_regen_plan<<<1, 1, 0, st>>>(E.ctl, qi ^ 1, E.capacity);
+  k_wf_regen<<<grid, 256, 0, st>>>(W, E.q[qi ^ 1]);
 }
 
 template <int MS, bool NEE>
@@ -1035,7 +988,7 @@ static int wf_run(WfParams W, WfEngine &E, cudaStream_t st, int *iterations) {
   int it = 0;
   for (int guard = 0; guard < 1 << 20; ++guard) {
     cudaGraphLaunch(E.graph, st);
-    g_launches += march_grid > 0 ? 32 : 24;
+    g_launches += march_grid > 0 ? 48 : 40;
     it += 8;
     cudaMemcpyAsync(E.h_ctl, E.ctl, sizeof(WfCtl), cudaMemcpyDeviceToHost, st);
     if (!cuda_ok(cudaStreamSynchronize(st), "wavefront iteration")) {
