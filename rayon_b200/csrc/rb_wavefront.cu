@@ -6,23 +6,24 @@
 //   thr    float4 (throughput xyz, -)                 L    float4 (radiance xyz, -)
 //   meta   int4   (pixel, sample, bounce, path key)   hit  float4 (t, prim, -, -)
 //   sn     float4 (SDF field normal xyz, material)    (written only on field hits)
-// One iteration is two launches over the live paths of queue A:
+// One iteration is these launches over the live paths of queue A:
 //   extend: trace each ray to its closest hit (traversal only: few registers,
 //           high occupancy for latency hiding);
 //   shade:  surface, material scatter, emission, next-event estimation,
 //           Russian roulette; a path that ends adds its radiance to the
-//           pixel (FP64 atomics: order-independent sums) and its slot takes
-//           the next work item (path regeneration). Survivors and new paths
-//           are written compacted into queue B: each warp ballots its lanes
-//           that produce a path, one lane reserves the warp's range with one
-//           atomic, lanes write at their rank.
-// Scenes with a smooth SDF field add a third launch between the two: extend
-// only collects each ray's field candidates (sorted by primitive index, one
-// 16-byte record per candidate: index and window [t0, t1]) and appends the
-// ray to a march list; march is a persistent kernel whose lanes each take a
-// ray from the list, advance it one sphere-tracing step per pass and take
-// the next ray as soon as theirs finishes, so a warp does not wait for its
-// slowest ray (a march takes from one to hundreds of steps).
+//           pixel (FP64 atomics: order-independent sums). Survivors are
+//           written compacted into queue B, each block's range claimed by
+//           its last warp to finish;
+//   regen:  the free slots of queue B take new camera paths for the next
+//           work items (path regeneration; a one-thread plan launch, then
+//           one thread per new path).
+// Scenes with a smooth SDF field add a launch between extend and shade:
+// extend only collects each ray's field candidates (a 256-bit set of SDF
+// primitives, or sorted 16-byte records of index and window [t0, t1]) and
+// appends the ray to a march list; march is a persistent kernel whose lanes
+// each take a ray from the list, advance it one sphere-tracing step per pass
+// and take the next ray as soon as theirs finishes, so a warp does not wait
+// for its slowest ray (a march takes from one to hundreds of steps).
 // The queues then swap. Work items are sample-major (consecutive lanes take
 // consecutive pixels of the same sample) so primary rays of a warp are
 // coherent and the accumulation atomics of a warp hit distinct pixels. The
