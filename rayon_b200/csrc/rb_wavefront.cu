@@ -939,7 +939,11 @@ static void wf_iteration(const WfParams &W, WfEngine &E, int qi, int grid, int m
     else k_wf_march<MS, false><<<march_grid, 256, tab, st>>>(W, E.q[qi], tab > 0 ? 1 : 0);
   }
   const int shade_grid = (E.capacity + WF_SHADE_THREADS - 1) / WF_SHADE_THREADS;
-  const size_t shade_sm = stack_smem_bytes(W.S.short_stack, WF_SHADE_THREADS);
+  // the shared stack's entries, within the 48 KB a block has beside the
+  // kernel's 20 KB of staged survivors (stack_init clamps the depth to what
+  // the launch provides: 8 entries by default, at most 13 here)
+  const size_t shade_sm = std::min(stack_smem_bytes(W.S.short_stack, WF_SHADE_THREADS),
+                                   (size_t)48 * 1024 - sizeof(float4) * 5 * WF_SHADE_THREADS - 256);
   k_wf_shade<MS, NEE><<<shade_grid, WF_SHADE_THREADS, shade_sm, st>>>(W, E.q[qi], E.q[qi ^ 1], qi);
   k_wf_regen_plan<<<1, 1, 0, st>>>(E.ctl, qi ^ 1, E.capacity);
   k_wf_regen<<<grid, 256, 0, st>>>(W, E.q[qi ^ 1]);
